@@ -1,0 +1,423 @@
+#!/usr/bin/env python
+"""bench.py -- SAR backprojection throughput on B200 (Gpixel*pulses/s).
+
+Workload (default): plain_large -- one 2048 x 2048 image from 1999 pulses x
+1024 samples (complex64), N_fft 4096, Taylor 30, seeded synthetic data with
+the reference's shapes (see halide-sar-app_b200/sarbp_b200/synth.py).
+
+A step is one backprojection call of the reference's `backprojection_cuda`
+interface: range compression (window, filter, pad, shift, FFT, shift) and
+per-pixel pulse accumulation into the complex128 image, all on the device.
+  value  inputs resident in HBM (sarbp_backprojection_device), K steps timed
+         with CUDA events on the launching stream; per-step inputs plus
+         outputs are ~250 MB, larger than the 126 MB L2
+  e2e    the host-buffer entry point (sarbp_backprojection) from pinned
+         host memory: host->device copies of phs, k_r, pos, r and the
+         device->host copy of the image inside the timed region
+
+Multi-GPU (torchrun, N > 1): every rank forms its own image (replicas, weak
+scaling); the time is the max over ranks.
+
+--impl reference times the reference algorithm's CPU implementation (the
+C restatement in oracle/, reference precision, all host threads) on a
+bounded pixel sample of the same workload; only rank 0 runs it.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "halide-sar-app_b200"))
+
+FP32_PER_UNIT = 18  # FP32-pipe instructions per pixel*pulse (algorithmic)
+SFU_PER_UNIT = 3    # SFU operations per pixel*pulse (algorithmic)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="plain_large")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="CPU work of the bounded CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--tile", default="", help="e.g. 32x32")
+    ap.add_argument("--chunk", type=int, default=0)
+    return ap.parse_args()
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu_id), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+                power.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
+                "power_w_max": max(power) if power else None, "reasons": sorted(reasons)}
+
+
+def gpu_uuid(torch, dev):
+    try:
+        return "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        return str(dev)
+
+
+def cpu_baseline_sample(data, seconds, nthreads=0):
+    """Times the reference-precision CPU oracle on a pixel sample of the
+    workload; range compression (all pulses) is charged pro rata."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.lib()
+    k32 = data["k_r"].astype(np.float32).astype(np.float64)
+    pos32 = data["pos"].astype(np.float32).astype(np.float64)
+    nu, nv, P = data["nu"], data["nv"], data["P"]
+    t0 = time.perf_counter()
+    Q = O.range_compress(data["phs"], k32, data["taylor"], data["N_fft"], O.MODE_REF, nthreads)
+    t_rc = time.perf_counter() - t0
+    rng = np.random.default_rng(0)
+    # calibrate on 512 pixels, then size the sample for `seconds`
+    idx = rng.choice(nu * nv, 512, replace=False)
+    t0 = time.perf_counter()
+    O.backproject(Q, data["S"], data["delta_r"], k32, pos32, data["r"], nu, nv, idx, O.MODE_REF, nthreads)
+    t_cal = time.perf_counter() - t0
+    n = int(min(nu * nv, max(512, 512 * seconds / max(t_cal, 1e-6))))
+    idx = rng.choice(nu * nv, n, replace=False)
+    t0 = time.perf_counter()
+    O.backproject(Q, data["S"], data["delta_r"], k32, pos32, data["r"], nu, nv, idx, O.MODE_REF, nthreads)
+    t_bp = time.perf_counter() - t0
+    t = t_bp + t_rc * n / (nu * nv)
+    return dict(value=n * P / t / 1e9, seconds=t_bp + t_rc, t_rc=t_rc, t_bp=t_bp, n_pix=n,
+                cores=O.max_threads())
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from sarbp_b200 import synth
+    data = synth.make(args.config, seed=2)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.lib()
+    k32 = data["k_r"].astype(np.float32).astype(np.float64)
+    pos32 = data["pos"].astype(np.float32).astype(np.float64)
+    nu, nv, P = data["nu"], data["nv"], data["P"]
+    rng = np.random.default_rng(0)
+    # per step: range compression of all pulses + a pixel sample sized so a
+    # step takes ~2 s; throughput charges range compression pro rata
+    t0 = time.perf_counter()
+    Q = O.range_compress(data["phs"], k32, data["taylor"], data["N_fft"], O.MODE_REF)
+    t_rc0 = time.perf_counter() - t0
+    idx = rng.choice(nu * nv, 256, replace=False)
+    t0 = time.perf_counter()
+    O.backproject(Q, data["S"], data["delta_r"], k32, pos32, data["r"], nu, nv, idx, O.MODE_REF)
+    t_cal = time.perf_counter() - t0
+    n = int(min(nu * nv, max(256, 256 * 2.0 / max(t_cal, 1e-6))))
+    units = t_tot = 0.0
+    for step in range(args.warmup + args.steps):
+        idx = rng.choice(nu * nv, n, replace=False)
+        t0 = time.perf_counter()
+        Q = O.range_compress(data["phs"], k32, data["taylor"], data["N_fft"], O.MODE_REF)
+        t1 = time.perf_counter()
+        O.backproject(Q, data["S"], data["delta_r"], k32, pos32, data["r"], nu, nv, idx, O.MODE_REF)
+        t2 = time.perf_counter()
+        if step >= args.warmup:
+            units += n * P
+            t_tot += (t2 - t1) + (t1 - t0) * n / (nu * nv)
+    value = units / t_tot / 1e9
+    cores = O.max_threads()
+    sample = ("%d random pixels x %d pulses per step, range compression of all %d pulses "
+              "charged pro rata (%d of %d pixels)" % (n, P, P, n, nu * nv))
+    out = {
+        "impl": "reference",
+        "metric": "Gpixel*pulses/s (2048^2 x 1999 backprojection)",
+        "value": value, "unit": "Gpixel*pulses/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_tot / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded, plain_large shapes)",
+        "config": config_block(data, world),
+        "cpu_baseline": {"value": value, "unit": "Gpixel*pulses/s", "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "Gpixel*pulses/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "reference CPU schedule restated in C (oracle/sarbp_oracle.c); the reference "
+                "itself needs Halide/FFTW/cnpy, which are not installable here",
+    }
+    print(json.dumps(out), flush=True)
+
+
+def config_block(data, world):
+    return {"workload": "%s: %dx%d image, %d pulses x %d samples, N_fft %d, Taylor %d" % (
+                data["name"], data["nu"], data["nv"], data["P"], data["S"], data["N_fft"],
+                data["taylor"]),
+            "image": [data["nu"], data["nv"]], "npulses": data["P"], "nsamples": data["S"],
+            "n_fft": data["N_fft"], "taylor": data["taylor"], "precision": "compat",
+            "parallelism": "replicas%d" % world,
+            "l2": "inputs+outputs ~250 MB per step (> 126 MB L2), no flush"}
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    import sarbp_b200 as sb
+    from sarbp_b200 import synth
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    data = synth.make(args.config, seed=2 + rank)
+    nu, nv, P, S = data["nu"], data["nv"], data["P"], data["S"]
+    units = float(nu) * nv * P
+
+    ctx = sb.Context(local_rank)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+    ffma_s, mufu_s = ctx.measure_peaks()
+
+    t_phs = torch.from_numpy(data["phs"].view(np.float32).copy()).to(dev)
+    t_k = torch.from_numpy(data["k_r"].astype(np.float32)).to(dev)
+    t_pos = torch.from_numpy(data["pos"].astype(np.float32)).to(dev)
+    t_r = torch.from_numpy(data["r"]).to(dev)
+    t_out = torch.empty((nv, nu, 2), dtype=torch.float64, device=dev)
+    tune = {}
+    if args.tile:
+        tune["tile"] = tuple(int(x) for x in args.tile.split("x"))
+    if args.chunk:
+        tune["pulse_chunk"] = args.chunk
+    job = sb.make_job(S, P, data["N_fft"], data["taylor"], nu, nv, data["delta_r"], t_phs.data_ptr(),
+                      t_k.data_ptr(), t_pos.data_ptr(), t_out.data_ptr(), r=t_r.data_ptr())
+
+    def barrier():
+        if world > 1:
+            dist.barrier(device_ids=[local_rank])
+
+    ctx.set_timing(True)
+    for _ in range(args.warmup):
+        ctx.run_jobs([job], **tune)
+    ctx.synchronize()
+
+    clocks = Clocks(gpu_uuid(torch, local_rank))
+    clocks.start()
+    time.sleep(0.3)
+    l0 = ctx.launch_count()
+    stage = []
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        ctx.run_jobs([job], **tune)
+        stage.append(ctx.last_stage_ms())
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    launches = ctx.launch_count() - l0
+    ms = ev0.elapsed_time(ev1)
+    ctx.synchronize()  # raises on a kernel status error
+    clk = clocks.stop()
+    ms_max = ms
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = world * units * args.steps / (ms_max * 1e-3) / 1e9
+
+    # output stage (dB + u8), outside the step: HBM-bound tail
+    t_u8 = torch.empty((nv, nu), dtype=torch.uint8, device=dev)
+    job_u8 = sb.make_job(S, P, data["N_fft"], data["taylor"], nu, nv, data["delta_r"], t_phs.data_ptr(),
+                         t_k.data_ptr(), t_pos.data_ptr(), t_out.data_ptr(), r=t_r.data_ptr(),
+                         out_u8=t_u8.data_ptr(), dB_min=data["db"][0], dB_max=data["db"][1])
+    u8_ms = []
+    for _ in range(3):
+        ctx.run_jobs([job_u8], **tune)
+        u8_ms.append(ctx.last_stage_ms()[3])
+    ctx.synchronize()
+
+    # ---- e2e through the host-buffer entry point, pinned host memory ----
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    h_phs, h_k = pin(data["phs"]), pin(data["k_r"].astype(np.float32))
+    h_pos, h_r = pin(data["pos"].astype(np.float32)), pin(data["r"])
+    h_u, h_v = data["u"], data["v"]
+    out_pinned = torch.empty((nv, nu, 2), dtype=torch.float64).pin_memory().numpy()
+
+    def e2e_call():
+        # same operator as sarbp_b200.Context.backprojection_cuda, writing into pinned memory
+        import ctypes
+        from sarbp_b200 import _lib
+        o = sb._opts(sb.PREC_COMPAT, **tune)
+        p = lambda a: ctypes.c_void_p(a.ctypes.data)
+        _lib.check(_lib.lib().sarbp_backprojection(
+            ctx.handle, p(h_phs), S, P, p(h_k), data["taylor"], data["N_fft"], data["delta_r"], p(h_u),
+            nu, p(h_v), nv, p(h_pos), p(h_r), p(out_pinned), ctypes.byref(o)))
+
+    e2e_call()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        e2e_call()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * units * args.e2e_steps / (e2e_ms * 1e-3) / 1e9
+    h2d = h_phs.nbytes + h_k.nbytes + h_pos.nbytes + h_r.nbytes
+    d2h = out_pinned.nbytes
+
+    # ---- roofline of the backprojection kernel (FP32 + SFU) ----
+    st = np.array(stage)
+    bp_ms = float(st[:, 2].mean())
+    rc_ms = float(st[:, 1].mean())
+    prep_ms = float(st[:, 0].mean())
+    bp_units_s = units / (bp_ms * 1e-3)
+    t_fp32 = FP32_PER_UNIT * units / ffma_s
+    t_sfu = SFU_PER_UNIT * units / mufu_s
+    bound = "sfu" if t_sfu >= t_fp32 else "fp32"
+    if bound == "sfu":
+        achieved, peak = SFU_PER_UNIT * bp_units_s / 1e12, mufu_s / 1e12
+    else:
+        achieved, peak = FP32_PER_UNIT * bp_units_s / 1e12, ffma_s / 1e12
+    rc_bytes = P * S * 8 + P * data["N_fft"] * 8
+    u8_bytes = nu * nv * (16 + 1)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    out = {
+        "metric": "Gpixel*pulses/s (2048^2 x 1999 backprojection)",
+        "value": value, "unit": "Gpixel*pulses/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (split-precision; f64 per-pulse set-up)",
+        "data": "synthetic (seeded, plain_large shapes)",
+        "config": config_block(data, world),
+        "gpu_launches": int(launches),
+        "stage_ms": {"setup": prep_ms, "range_compress": rc_ms, "backproject": bp_ms,
+                     "db_u8": float(np.mean(u8_ms))},
+        "roofline": {"bound": bound, "achieved": achieved, "peak": peak, "unit": "Tops/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "bp_tile_kernel",
+                     "per_unit": "%d FP32 instr + %d SFU ops per pixel*pulse" % (FP32_PER_UNIT, SFU_PER_UNIT),
+                     "peak_source": "measured in this run: FFMA / MUFU chain microkernels",
+                     "fp32": {"achieved": FP32_PER_UNIT * bp_units_s / 1e12, "peak": ffma_s / 1e12,
+                              "frac": FP32_PER_UNIT * bp_units_s / ffma_s},
+                     "sfu": {"achieved": SFU_PER_UNIT * bp_units_s / 1e12, "peak": mufu_s / 1e12,
+                             "frac": SFU_PER_UNIT * bp_units_s / mufu_s}},
+        "roofline_hbm": {
+            "range_compress": {"bound": "hbm", "achieved": rc_bytes / (rc_ms * 1e-3) / 1e9,
+                               "peak": hbm_peak, "unit": "GB/s",
+                               "frac": rc_bytes / (rc_ms * 1e-3) / 1e9 / hbm_peak,
+                               "bytes": rc_bytes},
+            "db_u8": {"bound": "hbm", "achieved": u8_bytes / (np.mean(u8_ms) * 1e-3) / 1e9,
+                      "peak": hbm_peak, "unit": "GB/s",
+                      "frac": u8_bytes / (np.mean(u8_ms) * 1e-3) / 1e9 / hbm_peak, "bytes": u8_bytes},
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s"},
+        "e2e": {"value": e2e_value, "unit": "Gpixel*pulses/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms / args.e2e_steps,
+                "steps": args.e2e_steps},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline_sample(data, args.cpu_seconds)
+        out["cpu_baseline"] = {"value": cb["value"], "unit": "Gpixel*pulses/s", "cores": cb["cores"],
+                               "kind": "port",
+                               "sample": "%d random pixels x %d pulses (reference-precision C oracle, "
+                                         "%d threads, %.1f s; range compression of all pulses "
+                                         "charged pro rata)" % (cb["n_pix"], P, cb["cores"],
+                                                                cb["seconds"])}
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args, rank, world)  # rank 0 only, no process group
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,76 @@
+// internal.h -- descriptors shared by the host pipeline and the kernels.
+//
+// One DevJob describes one image-formation job in device memory: the
+// caller's inputs, the library's per-job scratch (range profiles, windows,
+// per-pulse geometry) and the outputs.  The host builds an array of them,
+// copies it to the device, and every kernel of a batch indexes it by job.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sarbp {
+
+constexpr int kMaxTaylorTerms = 64;  // n_bar - 1 <= 64  (S_L up to ~150 dB)
+constexpr int kMinLogN = 4;          // N_fft in [16, 16384]
+constexpr int kMaxLogN = 14;
+
+// status bits written by kernels into DevJob::status
+constexpr int kStatusTileTooWide = 1;   // range window of a tile exceeds smem
+constexpr int kStatusNonFinite = 2;     // non-finite pixel or pulse geometry
+constexpr int kStatusNearField = 4;     // pulse closer than the tile radius
+
+// per-job words the kernels write; kept contiguous for one status read-back
+struct JobScalars {
+    unsigned long long maxabs;  // bits of max |z| (f64, non-negative)
+    double k_c;                 // k_r[S/2] by precision mode (prep kernel)
+    int status;                 // kStatus* bits
+    int pad[3];
+};
+
+struct DevJob {
+    // sizes
+    int S, P, N, nu, nv;
+    int precision;
+    int tiles_x, tiles_y;
+    int tile_x, tile_y;
+    int logN;
+    int n_taylor;  // n_bar - 1 coefficients (same for both axes)
+    // caller inputs (device)
+    const float2 *phs;    // [P][S]
+    const float *k_r32;   // [S]
+    const double *k_r64;  // [S] or null
+    const float *pos32;   // [P][3]
+    const double *pos64;  // [P][3] or null
+    const double *r;      // SoA [3][nu*nv] or null (grid form)
+    const double *u, *v;  // grid form
+    double uh[3], vh[3];
+    // library scratch (device)
+    float2 *Q;            // [P][N] range profiles
+    float *filt;          // [S]  |k_r|
+    float *wS;            // [S]  sample window
+    float *wP;            // [P]  pulse window
+    double4 *pulse;       // [P]  (x, y, z, |pos|) by precision mode
+    JobScalars *sc;       // max|z|, k_c, status (written by the kernels)
+    // constants
+    double delta_r, lsa, lsr, inv_lsr;
+    double taylor_F[kMaxTaylorTerms];
+    // outputs
+    double2 *out;         // [nv][nu]
+    uint8_t *out_u8;      // [nv][nu] or null
+    double dB_min, dB_max;
+};
+
+// (job, tile) work item of the persistent backprojection launch
+struct WorkItem {
+    int job;
+    int tile;
+};
+
+// one row of a batched range-compression launch
+struct RowItem {
+    int job;
+    int pulse;
+};
+
+}  // namespace sarbp

@@ -1,0 +1,53 @@
+// kernels.h -- launch wrappers of the device kernels (host-callable).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "internal.h"
+#include "sarbp_b200.h"
+
+#define SARBP_PREC_COMPAT_ SARBP_PREC_COMPAT
+#define SARBP_PREC_PRECISE_ SARBP_PREC_PRECISE
+#define SARBP_PREC_NAIVE_ SARBP_PREC_NAIVE
+
+namespace sarbp {
+
+// prep.cu
+void launch_prep(const DevJob *d_jobs, int njobs, cudaStream_t st);
+
+// range_compress.cu
+int twiddle_table_size(int logN);
+void fill_twiddle_table(int logN, float2 *host);
+cudaError_t launch_range_compress(int logN, const DevJob *d_jobs, const RowItem *d_rows, int nrows,
+                                  const float2 *d_tw, cudaStream_t st);
+cudaError_t init_range_compress_attributes();
+
+// backproject.cu
+struct BpLaunch {
+    int tile_x, tile_y;
+    int stage_cap;   // float4 entries of the staging buffer
+    int cmax;        // max pulses per chunk
+    int persistent;  // 1: grid = resident CTAs pulling items from *counter
+    int grid;        // CTAs when persistent
+};
+bool bp_tile_supported(int tile_x, int tile_y);
+size_t bp_smem_bytes(const BpLaunch &L);
+int bp_max_active_blocks(const BpLaunch &L);
+cudaError_t init_backproject_attributes();
+cudaError_t launch_backproject(const BpLaunch &L, const DevJob *d_jobs, const WorkItem *d_items,
+                               int nitems, int *d_counter, cudaStream_t st);
+cudaError_t launch_backproject_naive(const DevJob *d_jobs, int job, int nu, int nv, cudaStream_t st);
+
+// peaks.cu
+cudaError_t measure_peaks(int num_sms, cudaStream_t st, double *ffma_per_s, double *mufu_per_s);
+
+// output.cu
+cudaError_t launch_maxabs(const double2 *img, long long n, unsigned long long *d_max, cudaStream_t st);
+cudaError_t launch_db_u8(const double2 *img, long long n, const unsigned long long *d_max,
+                         double *dB, uint8_t *u8, double dB_min, double dB_max, cudaStream_t st);
+cudaError_t launch_u8_from_db(const double *dB, long long n, double dB_min, double dB_max,
+                              uint8_t *u8, cudaStream_t st);
+// u8 images of every job of a batch that asked for one (uses DevJob::maxabs)
+cudaError_t launch_batch_u8(const DevJob *d_jobs, int njobs, cudaStream_t st);
+
+}  // namespace sarbp

@@ -1,0 +1,112 @@
+// output.cu -- dB and u8 output stages (img_output.cpp:10-52).
+//
+//   m   = max |z| over the image               (img_output.cpp:23-24)
+//   dB  = 10 * log(|z| / m) / log(10)          (img_output.cpp:26, util.h:56-58;
+//         log(Expr(10)) has an integer argument, so Halide takes it in f32)
+//   u8  = trunc(clamp((clamp(dB, lo, hi) - lo) / (hi - lo) * 255, 0, 255))
+//                                              (img_output.cpp:48-51, signal.h:55-57)
+// All HBM-bound; the fused form reads the complex image once and writes the
+// u8 (and optionally the f64 dB) image, using the max|z| that the
+// backprojection epilogue already reduced.
+#include "internal.h"
+#include "kernels.h"
+
+namespace sarbp {
+
+namespace {
+
+constexpr double kLn10F32 = 2.302585124969482421875;  // logf(10.0f)
+
+__device__ __forceinline__ uint8_t to_u8(double v, double lo, double hi) {
+    if (v != v) v = lo;
+    v = fmin(fmax(v, lo), hi);
+    double n = (v - lo) / (hi - lo) * 255.0;
+    n = fmin(fmax(n, 0.0), 255.0);
+    return (uint8_t)n;
+}
+
+__global__ void maxabs_kernel(const double2 *__restrict__ img, long long n,
+                              unsigned long long *__restrict__ out) {
+    double m = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double2 z = img[i];
+        m = fmax(m, sqrt(z.x * z.x + z.y * z.y));
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ double s[32];
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, s[w]);
+        atomicMax(out, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+__global__ void db_u8_kernel(const double2 *__restrict__ img, long long n,
+                             const unsigned long long *__restrict__ maxbits, double *__restrict__ dB,
+                             uint8_t *__restrict__ u8, double lo, double hi) {
+    const double m = __longlong_as_double((long long)*maxbits);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double2 z = img[i];
+        const double a = sqrt(z.x * z.x + z.y * z.y);
+        const double d = 10.0 * (log(a / m) / kLn10F32);
+        if (dB) dB[i] = d;
+        if (u8) u8[i] = to_u8(d, lo, hi);
+    }
+}
+
+__global__ void u8_from_db_kernel(const double *__restrict__ dB, long long n, double lo, double hi,
+                                  uint8_t *__restrict__ u8) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        u8[i] = to_u8(dB[i], lo, hi);
+}
+
+// blockIdx.y = job; jobs without an u8 output return at once
+__global__ void batch_u8_kernel(const DevJob *__restrict__ jobs) {
+    const DevJob &jb = jobs[blockIdx.y];
+    if (!jb.out_u8) return;
+    const double m = __longlong_as_double((long long)jb.sc->maxabs);
+    const long long n = (long long)jb.nu * jb.nv;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double2 z = jb.out[i];
+        const double a = sqrt(z.x * z.x + z.y * z.y);
+        jb.out_u8[i] = to_u8(10.0 * (log(a / m) / kLn10F32), jb.dB_min, jb.dB_max);
+    }
+}
+
+int grid_for(long long n) {
+    long long b = (n + 255) / 256;
+    if (b > 148 * 16) b = 148 * 16;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+}  // namespace
+
+cudaError_t launch_maxabs(const double2 *img, long long n, unsigned long long *d_max, cudaStream_t st) {
+    maxabs_kernel<<<grid_for(n), 256, 0, st>>>(img, n, d_max);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_db_u8(const double2 *img, long long n, const unsigned long long *d_max, double *dB,
+                         uint8_t *u8, double lo, double hi, cudaStream_t st) {
+    db_u8_kernel<<<grid_for(n), 256, 0, st>>>(img, n, d_max, dB, u8, lo, hi);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_u8_from_db(const double *dB, long long n, double lo, double hi, uint8_t *u8,
+                              cudaStream_t st) {
+    u8_from_db_kernel<<<grid_for(n), 256, 0, st>>>(dB, n, lo, hi, u8);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_u8(const DevJob *d_jobs, int njobs, cudaStream_t st) {
+    batch_u8_kernel<<<dim3(64, njobs), 256, 0, st>>>(d_jobs);
+    return cudaGetLastError();
+}
+
+}  // namespace sarbp

@@ -1,0 +1,426 @@
+// runner.cpp -- validation, scratch layout and launch sequence of a batch.
+#include "runner.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "host_math.h"
+
+namespace sarbp {
+
+namespace {
+thread_local std::string g_error;
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+bool is_pow2(long long n) { return n > 0 && (n & (n - 1)) == 0; }
+int ilog2i(long long n) {
+    int l = 0;
+    while ((1ll << l) < n) ++l;
+    return l;
+}
+
+struct JobLayout {
+    size_t Q, filt, wS, wP, pulse, end;
+};
+
+JobLayout layout_of(const sarbp_job &j, size_t base) {
+    JobLayout L;
+    size_t o = base;
+    L.Q = o;      o = align_up(o + (size_t)j.npulses * j.n_fft * sizeof(float2), 256);
+    L.filt = o;   o = align_up(o + (size_t)j.nsamples * sizeof(float), 256);
+    L.wS = o;     o = align_up(o + (size_t)j.nsamples * sizeof(float), 256);
+    L.wP = o;     o = align_up(o + (size_t)j.npulses * sizeof(float), 256);
+    L.pulse = o;  o = align_up(o + (size_t)j.npulses * sizeof(double4), 256);
+    L.end = o;
+    return L;
+}
+
+int precision_of(const sarbp_job &j, const sarbp_opts *o) {
+    if (j.precision >= 0) return j.precision;
+    return o ? o->precision : SARBP_PREC_COMPAT;
+}
+
+int validate(const sarbp_job &j, int prec, int idx, bool rc_only) {
+    auto bad = [&](const std::string &what) {
+        return fail(SARBP_ERR_INVALID, "job " + std::to_string(idx) + ": " + what);
+    };
+    if (j.nsamples < 1 || j.npulses < 1) return bad("nsamples and npulses must be >= 1");
+    if (!rc_only && (j.nu < 1 || j.nv < 1)) return bad("image extents nu and nv must be >= 1");
+    if ((long long)j.nu * j.nv > (1ll << 31)) return bad("image larger than 2^31 pixels");
+    if (!is_pow2(j.n_fft) || j.n_fft < (1 << kMinLogN) || j.n_fft > (1 << kMaxLogN))
+        return fail(SARBP_ERR_UNSUPPORTED, "job " + std::to_string(idx) +
+                                               ": N_fft must be a power of two in [16, 16384], got " +
+                                               std::to_string(j.n_fft));
+    if (j.taylor_s_l < 1) return bad("taylor must be >= 1");
+    if (!(std::isfinite(j.delta_r))) return bad("delta_r must be finite");
+    if (prec != SARBP_PREC_COMPAT && prec != SARBP_PREC_PRECISE && prec != SARBP_PREC_NAIVE)
+        return bad("unknown precision mode");
+    if (!j.phs) return bad("phs is NULL");
+    if (!j.k_r && !(prec == SARBP_PREC_PRECISE && j.k_r64)) return bad("k_r is NULL");
+    if (!j.pos && !(prec == SARBP_PREC_PRECISE && j.pos64)) return bad("pos is NULL");
+    if (!rc_only && !j.r && !(j.u && j.v)) return bad("pixel positions: r, or u and v, are required");
+    if (!rc_only && !j.output_img) return bad("output_img is NULL");
+    if (j.out_u8 && !(j.dB_min < j.dB_max)) return bad("dB_min < dB_max is required for the u8 image");
+    const std::vector<double> F = taylor_coefficients(j.taylor_s_l);
+    if ((int)F.size() > kMaxTaylorTerms) return bad("taylor side-lobe level too large (n_bar > 65)");
+    for (double f : F)
+        if (!std::isfinite(f))
+            return bad("taylor " + std::to_string(j.taylor_s_l) +
+                       " dB: the window formula of signal.h:39-41 divides by zero for side-lobe "
+                       "levels above 30 dB (its F_m denominator uses Int32 division)");
+    const double lsa = std::floor((double)(-j.nsamples) * j.delta_r / 2);
+    const double lsb = std::floor((double)j.nsamples * j.delta_r / 2);
+    if (!(lsb > lsa)) return bad("range axis is empty: floor(S*delta_r/2) <= floor(-S*delta_r/2)");
+    return SARBP_OK;
+}
+}  // namespace
+
+void set_error(const std::string &msg) { g_error = msg; }
+int fail(int code, const std::string &msg) {
+    g_error = msg;
+    return code;
+}
+int cuda_fail(cudaError_t e, const char *what) {
+    g_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? SARBP_ERR_NOMEM : SARBP_ERR_CUDA;
+}
+const char *last_error_cstr() { return g_error.c_str(); }
+
+cudaError_t DeviceBuffer::ensure(size_t bytes, cudaStream_t st) {
+    if (bytes <= cap) return cudaSuccess;
+    if (ptr) {
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return e;
+        cudaFree(ptr);
+        ptr = nullptr;
+        cap = 0;
+    }
+    const size_t want = align_up(bytes + bytes / 8, 1 << 20);
+    cudaError_t e = cudaMalloc(&ptr, want);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        return e;
+    }
+    cap = want;
+    return cudaSuccess;
+}
+void DeviceBuffer::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+}
+
+cudaError_t PinnedBuffer::ensure(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    cap = 0;
+    const size_t want = align_up(bytes + bytes / 4, 1 << 16);
+    cudaError_t e = cudaMallocHost(&ptr, want);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        return e;
+    }
+    cap = want;
+    return cudaSuccess;
+}
+void PinnedBuffer::release() {
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    cap = 0;
+}
+
+cudaError_t DeviceInfo::twiddle(int logN, float2 **out) {
+    auto it = twiddles.find(logN);
+    if (it != twiddles.end()) {
+        *out = it->second;
+        return cudaSuccess;
+    }
+    const int n = std::max(1, twiddle_table_size(logN));
+    std::vector<float2> h(n);
+    fill_twiddle_table(logN, h.data());
+    float2 *d = nullptr;
+    cudaError_t e = cudaMalloc(&d, n * sizeof(float2));
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpy(d, h.data(), n * sizeof(float2), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        return e;
+    }
+    twiddles[logN] = d;
+    *out = d;
+    return cudaSuccess;
+}
+cudaError_t DeviceInfo::record(int i, cudaStream_t st) {
+    if (!timing) return cudaSuccess;
+    if (!ev[i]) {
+        cudaError_t e = cudaEventCreate(&ev[i]);
+        if (e != cudaSuccess) return e;
+    }
+    ev_recorded[i] = true;
+    return cudaEventRecord(ev[i], st);
+}
+
+void DeviceInfo::release() {
+    for (int i = 0; i < 5; ++i)
+        if (ev[i]) cudaEventDestroy(ev[i]);
+    for (auto &kv : twiddles) cudaFree(kv.second);
+    twiddles.clear();
+}
+
+BpLaunch default_launch(const sarbp_opts *opts, int num_sms) {
+    BpLaunch L;
+    L.tile_x = 32;
+    L.tile_y = 32;
+    L.stage_cap = 2048;
+    L.cmax = 64;
+    L.persistent = 1;
+    if (opts) {
+        if (opts->tile_x > 0 && opts->tile_y > 0) {
+            L.tile_x = opts->tile_x;
+            L.tile_y = opts->tile_y;
+        }
+        if (opts->pulse_chunk > 0) L.cmax = std::min(256, std::max(4, opts->pulse_chunk));
+        L.persistent = opts->persistent == 2 ? 0 : 1;
+        if (opts->stage_cap > 0) L.stage_cap = std::max(64, std::min(12288, opts->stage_cap));
+    }
+    L.cmax = (L.cmax + 3) / 4 * 4;
+    L.grid = num_sms;
+    return L;
+}
+
+size_t Runner::job_scratch_bytes(const sarbp_job &j) { return layout_of(j, 0).end; }
+
+Runner::~Runner() {
+    scratch_.release();
+    meta_.release();
+    host_meta_.release();
+    if (meta_done_) cudaEventDestroy(meta_done_);
+}
+
+int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cudaStream_t st,
+                    void *q_out) {
+    const bool rc_only = q_out != nullptr;
+    if (njobs < 1 || !jobs) return fail(SARBP_ERR_INVALID, "no jobs");
+    BpLaunch L = default_launch(opts, dev_->num_sms);
+    if (!bp_tile_supported(L.tile_x, L.tile_y))
+        return fail(SARBP_ERR_INVALID, "unsupported pixel tile " + std::to_string(L.tile_x) + "x" +
+                                           std::to_string(L.tile_y));
+    std::vector<int> prec(njobs);
+    for (int i = 0; i < njobs; ++i) {
+        prec[i] = precision_of(jobs[i], opts);
+        int rc = validate(jobs[i], prec[i], i, rc_only);
+        if (rc) return rc;
+    }
+    if (!meta_done_) {
+        cudaError_t e = cudaEventCreateWithFlags(&meta_done_, cudaEventDisableTiming);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaEventCreate");
+    }
+    // ---- scratch layout: JobScalars block first, then per-job arrays ----
+    size_t off = align_up((size_t)njobs * sizeof(JobScalars), 256);
+    std::vector<JobLayout> lay(njobs);
+    for (int i = 0; i < njobs; ++i) {
+        lay[i] = layout_of(jobs[i], off);
+        off = lay[i].end;
+    }
+    cudaError_t e = scratch_.ensure(off, st);
+    if (e != cudaSuccess) return cuda_fail(e, "allocating scratch");
+    char *sbase = static_cast<char *>(scratch_.ptr);
+
+    // ---- rows grouped by N_fft, work items longest first ----
+    std::map<int, std::vector<RowItem>> rows;
+    std::vector<WorkItem> items;
+    std::vector<int> naive;
+    for (int i = 0; i < njobs; ++i) {
+        const int logN = ilog2i(jobs[i].n_fft);
+        auto &v = rows[logN];
+        for (int p = 0; p < jobs[i].npulses; ++p) v.push_back(RowItem{i, p});
+        if (rc_only) continue;
+        if (prec[i] == SARBP_PREC_NAIVE) {
+            naive.push_back(i);
+            continue;
+        }
+        const int tx = (jobs[i].nu + L.tile_x - 1) / L.tile_x;
+        const int ty = (jobs[i].nv + L.tile_y - 1) / L.tile_y;
+        for (int t = 0; t < tx * ty; ++t) items.push_back(WorkItem{i, t});
+    }
+    std::stable_sort(items.begin(), items.end(), [&](const WorkItem &a, const WorkItem &b) {
+        return jobs[a.job].npulses > jobs[b.job].npulses;
+    });
+    size_t nrows_total = 0;
+    for (auto &kv : rows) nrows_total += kv.second.size();
+
+    // ---- meta block: [DevJob][RowItem...][WorkItem...][counter] ----
+    const size_t o_jobs = 0;
+    const size_t o_rows = align_up(o_jobs + (size_t)njobs * sizeof(DevJob), 256);
+    const size_t o_items = align_up(o_rows + nrows_total * sizeof(RowItem), 256);
+    const size_t o_cnt = align_up(o_items + items.size() * sizeof(WorkItem), 256);
+    const size_t meta_bytes = o_cnt + 256;
+    // the previous batch's descriptor copy must have left host_meta_
+    e = cudaEventSynchronize(meta_done_);
+    if (e != cudaSuccess) return cuda_fail(e, "waiting for the previous batch");
+    e = host_meta_.ensure(meta_bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "allocating pinned descriptors");
+    e = meta_.ensure(meta_bytes, st);
+    if (e != cudaSuccess) return cuda_fail(e, "allocating device descriptors");
+    char *h = static_cast<char *>(host_meta_.ptr);
+    char *d = static_cast<char *>(meta_.ptr);
+    std::memset(h, 0, meta_bytes);
+
+    DevJob *hj = reinterpret_cast<DevJob *>(h + o_jobs);
+    for (int i = 0; i < njobs; ++i) {
+        const sarbp_job &j = jobs[i];
+        DevJob &dj = hj[i];
+        dj.S = j.nsamples;
+        dj.P = j.npulses;
+        dj.N = j.n_fft;
+        dj.nu = j.nu;
+        dj.nv = j.nv;
+        dj.precision = prec[i];
+        dj.tile_x = L.tile_x;
+        dj.tile_y = L.tile_y;
+        dj.tiles_x = (j.nu + L.tile_x - 1) / L.tile_x;
+        dj.tiles_y = (j.nv + L.tile_y - 1) / L.tile_y;
+        dj.logN = ilog2i(j.n_fft);
+        const std::vector<double> F = taylor_coefficients(j.taylor_s_l);
+        dj.n_taylor = (int)F.size();
+        for (size_t k = 0; k < F.size(); ++k) dj.taylor_F[k] = F[k];
+        dj.phs = reinterpret_cast<const float2 *>(j.phs);
+        dj.k_r32 = j.k_r;
+        dj.k_r64 = j.k_r64;
+        dj.pos32 = j.pos;
+        dj.pos64 = j.pos64;
+        if (prec[i] == SARBP_PREC_PRECISE) {
+            if (!dj.k_r64 && !dj.k_r32) return fail(SARBP_ERR_INVALID, "k_r missing");
+            if (!dj.k_r32) dj.k_r32 = nullptr;
+        }
+        dj.r = j.r;
+        dj.u = j.u;
+        dj.v = j.v;
+        for (int k = 0; k < 3; ++k) {
+            dj.uh[k] = j.u_hat[k];
+            dj.vh[k] = j.v_hat[k];
+        }
+        dj.Q = reinterpret_cast<float2 *>(sbase + lay[i].Q);
+        dj.filt = reinterpret_cast<float *>(sbase + lay[i].filt);
+        dj.wS = reinterpret_cast<float *>(sbase + lay[i].wS);
+        dj.wP = reinterpret_cast<float *>(sbase + lay[i].wP);
+        dj.pulse = reinterpret_cast<double4 *>(sbase + lay[i].pulse);
+        dj.sc = reinterpret_cast<JobScalars *>(sbase) + i;
+        dj.delta_r = j.delta_r;
+        // backprojection.cpp:120 and :53: lsa = floor(-S*dr/2), lsb = floor(S*dr/2),
+        // lsr = (lsb - lsa) / (N_fft - 1)
+        dj.lsa = std::floor((double)(-j.nsamples) * j.delta_r / 2);
+        const double lsb = std::floor((double)j.nsamples * j.delta_r / 2);
+        dj.lsr = (lsb - dj.lsa) / (double)(j.n_fft - 1);
+        dj.inv_lsr = 1.0 / dj.lsr;
+        dj.out = reinterpret_cast<double2 *>(j.output_img);
+        dj.out_u8 = j.out_u8;
+        dj.dB_min = j.dB_min;
+        dj.dB_max = j.dB_max;
+    }
+    RowItem *hr = reinterpret_cast<RowItem *>(h + o_rows);
+    std::vector<std::pair<int, size_t>> row_groups;  // (logN, first row)
+    size_t rpos = 0;
+    for (auto &kv : rows) {
+        row_groups.push_back({kv.first, rpos});
+        std::memcpy(hr + rpos, kv.second.data(), kv.second.size() * sizeof(RowItem));
+        rpos += kv.second.size();
+    }
+    std::memcpy(h + o_items, items.data(), items.size() * sizeof(WorkItem));
+
+    e = cudaMemcpyAsync(d, h, meta_bytes, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(e, "copying descriptors");
+    e = cudaEventRecord(meta_done_, st);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+
+    const DevJob *d_jobs = reinterpret_cast<const DevJob *>(d + o_jobs);
+    const RowItem *d_rows = reinterpret_cast<const RowItem *>(d + o_rows);
+    const WorkItem *d_items = reinterpret_cast<const WorkItem *>(d + o_items);
+    int *d_cnt = reinterpret_cast<int *>(d + o_cnt);
+
+    // twiddle tables first (a one-time synchronous upload per N_fft)
+    for (size_t g = 0; g < row_groups.size(); ++g) {
+        float2 *tw = nullptr;
+        e = dev_->twiddle(row_groups[g].first, &tw);
+        if (e != cudaSuccess) return cuda_fail(e, "twiddle table");
+    }
+    for (int k = 0; k < 5; ++k) dev_->ev_recorded[k] = false;
+    if ((e = dev_->record(0, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    launch_prep(d_jobs, njobs, st);
+    dev_->launches++;
+    if ((e = dev_->record(1, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    for (size_t g = 0; g < row_groups.size(); ++g) {
+        const int logN = row_groups[g].first;
+        const size_t first = row_groups[g].second;
+        const size_t count = rows[logN].size();
+        float2 *tw = nullptr;
+        e = dev_->twiddle(logN, &tw);
+        if (e != cudaSuccess) return cuda_fail(e, "twiddle table");
+        e = launch_range_compress(logN, d_jobs, d_rows + first, (int)count, tw, st);
+        if (e != cudaSuccess) return cuda_fail(e, "range compression launch");
+        dev_->launches++;
+    }
+    if ((e = dev_->record(2, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    if (rc_only) {
+        e = cudaMemcpyAsync(q_out, hj[0].Q, (size_t)jobs[0].npulses * jobs[0].n_fft * sizeof(float2),
+                            cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return cuda_fail(e, "copying range profiles");
+        last_njobs_ = njobs;
+        last_status_dev_ = reinterpret_cast<int *>(sbase);
+        return SARBP_OK;
+    }
+    if (!items.empty()) {
+        if (L.persistent) {
+            const int occ = bp_max_active_blocks(L);
+            if (occ < 1) return fail(SARBP_ERR_CUDA, "backprojection kernel does not fit on an SM");
+            L.grid = std::min<long long>((long long)occ * dev_->num_sms, (long long)items.size());
+        }
+        e = launch_backproject(L, d_jobs, d_items, (int)items.size(), d_cnt, st);
+        if (e != cudaSuccess) return cuda_fail(e, "backprojection launch");
+        dev_->launches++;
+    }
+    for (int i : naive) {
+        e = launch_backproject_naive(d_jobs, i, jobs[i].nu, jobs[i].nv, st);
+        if (e != cudaSuccess) return cuda_fail(e, "naive backprojection launch");
+        dev_->launches++;
+    }
+    if ((e = dev_->record(3, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    bool any_u8 = false;
+    for (int i = 0; i < njobs; ++i) any_u8 = any_u8 || jobs[i].out_u8;
+    if (any_u8) {
+        e = launch_batch_u8(d_jobs, njobs, st);
+        if (e != cudaSuccess) return cuda_fail(e, "u8 launch");
+        dev_->launches++;
+        if ((e = dev_->record(4, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    }
+    last_njobs_ = njobs;
+    last_status_dev_ = reinterpret_cast<int *>(sbase);
+    return SARBP_OK;
+}
+
+int Runner::check_status(cudaStream_t st) {
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "synchronising the stream");
+    if (!last_status_dev_ || last_njobs_ == 0) return SARBP_OK;
+    std::vector<JobScalars> sc(last_njobs_);
+    e = cudaMemcpy(sc.data(), last_status_dev_, sc.size() * sizeof(JobScalars), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "reading job status");
+    for (int i = 0; i < last_njobs_; ++i) {
+        const int s = sc[i].status;
+        if (s & kStatusNonFinite)
+            return fail(SARBP_ERR_GEOMETRY, "job " + std::to_string(i) +
+                                                ": non-finite pixel or antenna position (those "
+                                                "pixels or pulses were left out)");
+        if (s & kStatusTileTooWide)
+            return fail(SARBP_ERR_GEOMETRY,
+                        "job " + std::to_string(i) +
+                            ": a pixel tile spans more range bins than fit on chip (pixel positions "
+                            "are not spatially compact); those tiles were left at zero");
+    }
+    return SARBP_OK;
+}
+
+}  // namespace sarbp

@@ -1,0 +1,84 @@
+// runner.h -- enqueues one batch of image-formation jobs on a stream.
+//
+// A Runner owns the device memory a batch needs besides the caller's
+// arrays: the job descriptors, row and work-item lists, and a grow-only
+// scratch arena for range profiles, windows and per-pulse geometry.  One
+// Runner serves one stream; the serving loop keeps several.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+#include "kernels.h"
+#include "sarbp_b200.h"
+
+namespace sarbp {
+
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    size_t cap = 0;
+    // Grows to at least `bytes`; synchronises `st` before freeing the old one.
+    cudaError_t ensure(size_t bytes, cudaStream_t st);
+    void release();
+};
+
+struct PinnedBuffer {
+    void *ptr = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes);
+    void release();
+};
+
+// Per-device constants shared by all runners of a context.
+struct DeviceInfo {
+    int device = 0;
+    int num_sms = 148;
+    std::map<int, float2 *> twiddles;  // logN -> device table
+    long long launches = 0;
+    // stage timing: events [0] before set-up, [1] after set-up, [2] after
+    // range compression, [3] after backprojection, [4] after u8
+    bool timing = false;
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    bool ev_recorded[5] = {false, false, false, false, false};
+    cudaError_t record(int i, cudaStream_t st);
+    cudaError_t twiddle(int logN, float2 **out);
+    void release();
+};
+
+class Runner {
+public:
+    explicit Runner(DeviceInfo *dev) : dev_(dev) {}
+    ~Runner();
+    // Validates and enqueues jobs on st.  Returns SARBP_OK or an error code
+    // (no device work is enqueued on a validation error).
+    // With q_out set, only range compression runs and job 0's profiles are
+    // copied there.
+    int enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cudaStream_t st,
+                void *q_out = nullptr);
+    // Waits for the last batch and reads the kernels' status words.
+    int check_status(cudaStream_t st);
+    // Device footprint of the library scratch a job needs (bytes).
+    static size_t job_scratch_bytes(const sarbp_job &j);
+
+private:
+    DeviceInfo *dev_;
+    DeviceBuffer scratch_, meta_;
+    PinnedBuffer host_meta_;
+    cudaEvent_t meta_done_ = nullptr;  // host_meta_ may be rewritten after this
+    int last_njobs_ = 0;
+    int *last_status_dev_ = nullptr;   // status words of the last batch
+    std::vector<int> status_host_;
+    std::vector<int> last_status_stride_;
+};
+
+BpLaunch default_launch(const sarbp_opts *opts, int num_sms);
+
+}  // namespace sarbp

@@ -1,0 +1,234 @@
+"""sarbp_b200 -- SAR backprojection on B200 (sm_100a), Python side.
+
+Mirrors the reference application's operator interface for the `-s cuda`
+path (ISI-apex/halide-sar-app):
+
+  backprojection_cuda(phs, k_r, taylor_s_l, N_fft, delta_r, u, v, pos, r)
+        -> output_img            (backprojection.cpp:35-46, sarbp.cpp:277)
+  img_output_to_dB(img) -> dB    (img_output.cpp:10-39)
+  img_output_u8(dB, dB_min, dB_max) -> u8   (img_output.cpp:41-52)
+  img_plane_create(...)          (ImgPlane.cpp:16-63)
+  taylor(num, S_L)               (signal.h:14-51)
+
+Arrays use the reference's memory layouts (see include/sarbp_b200.h); the
+image comes back as complex128 [nv, nu] with the reference's row flip.
+All compute runs through libsarbp_b200.so; there is no CPU path.
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from ._lib import (ERR_ADMISSION, ERR_CUDA, ERR_GEOMETRY, ERR_INVALID, ERR_NOMEM, ERR_STATE,
+                   ERR_TIMEOUT, ERR_UNSUPPORTED, OK, PREC_COMPAT, PREC_NAIVE, PREC_PRECISE, Job,
+                   Opts, SarbpError, check, lib)
+
+__all__ = [
+    "Context", "Job", "Opts", "SarbpError", "PREC_COMPAT", "PREC_PRECISE", "PREC_NAIVE",
+    "n_fft_for", "taylor", "img_plane_create", "img_plane_dims", "pixel_locs", "version",
+]
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else ctypes.c_void_p(0)
+
+
+def version():
+    return lib().sarbp_version().decode()
+
+
+def n_fft_for(nsamples, upsample):
+    """FFT width of sarbp.cpp:258: 2^(floor(log2(nsamples*upsample)) + 1)."""
+    return int(math.pow(2, int(math.log2(nsamples * upsample)) + 1))
+
+
+def taylor(num, S_L):
+    out = np.empty(num, np.float64)
+    check(lib().sarbp_taylor(int(num), float(S_L), _ptr(out)))
+    return out
+
+
+def img_plane_dims(nsamples, npulses, upsample=True):
+    nu, nv = ctypes.c_int(), ctypes.c_int()
+    check(lib().sarbp_img_plane_dims(int(nsamples), int(npulses), int(bool(upsample)),
+                                     ctypes.byref(nu), ctypes.byref(nv)))
+    return nu.value, nv.value
+
+
+def img_plane_create(nsamples, npulses, delta_r, R_c, n_hat=(0.0, 0.0, 1.0), res_factor=1.0,
+                     aspect=1.0, upsample=True, with_pixel_locs=True):
+    """ImgPlane.cpp:16-63; returns dict(nu, nv, d_u, d_v, u, v, k_u, k_v, u_hat,
+    v_hat[, pixel_locs SoA [3, nu*nv]])."""
+    nu, nv = img_plane_dims(nsamples, npulses, upsample)
+    R_c = np.ascontiguousarray(R_c, np.float32)
+    n_hat = np.ascontiguousarray(n_hat, np.float32)
+    o = {k: np.empty(n, np.float64) for k, n in
+         (("u", nu), ("v", nv), ("k_u", nu), ("k_v", nv), ("u_hat", 3), ("v_hat", 3))}
+    pl = np.empty((3, nu * nv), np.float64) if with_pixel_locs else None
+    du, dv = ctypes.c_double(), ctypes.c_double()
+    check(lib().sarbp_img_plane(int(nsamples), int(npulses), float(delta_r), _ptr(R_c), _ptr(n_hat),
+                                float(res_factor), float(aspect), int(bool(upsample)),
+                                ctypes.cast(ctypes.byref(du), ctypes.c_void_p),
+                                ctypes.cast(ctypes.byref(dv), ctypes.c_void_p),
+                                *[_ptr(o[k]) for k in ("u", "v", "k_u", "k_v", "u_hat", "v_hat")],
+                                _ptr(pl)))
+    o.update(nu=nu, nv=nv, d_u=du.value, d_v=dv.value)
+    if pl is not None:
+        o["pixel_locs"] = pl
+    return o
+
+
+def pixel_locs(u, v, u_hat, v_hat):
+    """img_plane.cpp:92-102: SoA [3, nu*nv], pixel i at u[i % nu], v[i // nu]."""
+    u = np.asarray(u, np.float64)
+    v = np.asarray(v, np.float64)
+    out = np.empty((3, u.size * v.size), np.float64)
+    for d in range(3):
+        out[d] = np.add.outer(v_hat[d] * v, u_hat[d] * u).ravel()
+    return out
+
+
+def _opts(precision=None, tile=None, pulse_chunk=0, persistent=0, stage_cap=0):
+    o = Opts()
+    o.precision = PREC_COMPAT if precision is None else int(precision)
+    if tile:
+        o.tile_x, o.tile_y = int(tile[0]), int(tile[1])
+    o.pulse_chunk = int(pulse_chunk)
+    o.persistent = int(persistent)
+    o.stage_cap = int(stage_cap)
+    return o
+
+
+class Context:
+    """One device context (device memory, stream, kernel launch counter)."""
+
+    def __init__(self, device=0):
+        self._h = ctypes.c_void_p()
+        check(lib().sarbp_ctx_create(int(device), ctypes.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            lib().sarbp_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, cuda_stream_handle):
+        check(lib().sarbp_ctx_set_stream(self._h, ctypes.c_void_p(cuda_stream_handle or 0)))
+
+    def synchronize(self):
+        check(lib().sarbp_ctx_synchronize(self._h))
+
+    def launch_count(self):
+        return int(lib().sarbp_ctx_launch_count(self._h))
+
+    def set_timing(self, on=True):
+        check(lib().sarbp_ctx_set_timing(self._h, int(bool(on))))
+
+    def last_stage_ms(self):
+        """(set-up, range compression, backprojection, u8) ms of the last batch."""
+        ms = (ctypes.c_float * 4)()
+        check(lib().sarbp_ctx_last_stage_ms(self._h, ms))
+        return tuple(float(x) for x in ms)
+
+    def measure_peaks(self):
+        """(FFMA instructions/s, MUFU ops/s) measured on this device."""
+        f, m = ctypes.c_double(), ctypes.c_double()
+        check(lib().sarbp_measure_peaks(self._h, ctypes.byref(f), ctypes.byref(m)))
+        return f.value, m.value
+
+    # ---- the reference's operators, host arrays ----
+    def backprojection_cuda(self, phs, k_r, taylor_s_l, N_fft, delta_r, u, v, pos, r,
+                            precision=None, **tune):
+        """Drop-in for the Halide pipeline backprojection_cuda.  phs complex64
+        [P, S]; k_r [S]; pos [P, 3]; r SoA [3, nu*nv]; returns complex128
+        [nv, nu].  f32 pos/k_r run with the reference's semantics
+        (PREC_COMPAT); f64 pos/k_r default to PREC_PRECISE."""
+        phs = np.ascontiguousarray(phs, np.complex64)
+        P, S = phs.shape
+        u = np.ascontiguousarray(u, np.float64)
+        v = np.ascontiguousarray(v, np.float64)
+        nu, nv = u.size, v.size
+        r = np.ascontiguousarray(r, np.float64)
+        if r.size != 3 * nu * nv:
+            raise SarbpError(ERR_INVALID, "r must hold 3*nu*nv values")
+        out = np.empty((nv, nu), np.complex128)
+        wide = np.asarray(pos).dtype == np.float64 or np.asarray(k_r).dtype == np.float64
+        if wide:
+            pos = np.ascontiguousarray(pos, np.float64)
+            k_r = np.ascontiguousarray(k_r, np.float64)
+            o = _opts(PREC_PRECISE if precision is None else precision, **tune)
+            fn = lib().sarbp_backprojection_f64
+        else:
+            pos = np.ascontiguousarray(pos, np.float32)
+            k_r = np.ascontiguousarray(k_r, np.float32)
+            o = _opts(PREC_COMPAT if precision is None else precision, **tune)
+            fn = lib().sarbp_backprojection
+        if pos.size != 3 * P or k_r.size != S:
+            raise SarbpError(ERR_INVALID, "pos must be [P, 3] and k_r [S]")
+        check(fn(self._h, _ptr(phs), S, P, _ptr(k_r), int(taylor_s_l), int(N_fft), float(delta_r),
+                 _ptr(u), nu, _ptr(v), nv, _ptr(pos), _ptr(r), _ptr(out), ctypes.byref(o)))
+        return out
+
+    def img_output_to_dB(self, img):
+        img = np.ascontiguousarray(img, np.complex128)
+        nv, nu = img.shape
+        out = np.empty((nv, nu), np.float64)
+        check(lib().sarbp_img_output_to_dB(self._h, _ptr(img), nu, nv, _ptr(out)))
+        return out
+
+    def img_output_u8(self, dB, dB_min, dB_max):
+        dB = np.ascontiguousarray(dB, np.float64)
+        nv, nu = dB.shape
+        out = np.empty((nv, nu), np.uint8)
+        check(lib().sarbp_img_output_u8(self._h, _ptr(dB), nu, nv, float(dB_min), float(dB_max),
+                                        _ptr(out)))
+        return out
+
+    def range_compress_device(self, job, q_out_ptr, precision=None):
+        """Writes the complex64 range profiles [P, N_fft] of `job` to q_out_ptr."""
+        o = _opts(precision)
+        check(lib().sarbp_range_compress_device(self._h, ctypes.byref(job), ctypes.byref(o),
+                                                ctypes.c_void_p(q_out_ptr)))
+
+    # ---- device-resident jobs (pointers from torch tensors or raw ints) ----
+    def run_jobs(self, jobs, precision=None, **tune):
+        """Enqueues a list of Job structs (device pointers) as one batch."""
+        arr = (Job * len(jobs))(*jobs)
+        o = _opts(precision, **tune)
+        if len(jobs) == 1:
+            check(lib().sarbp_backprojection_device(self._h, arr, ctypes.byref(o)))
+        else:
+            check(lib().sarbp_batch_device(self._h, arr, len(jobs), ctypes.byref(o)))
+
+
+def make_job(nsamples, npulses, n_fft, taylor_s_l, nu, nv, delta_r, phs, k_r, pos, output_img,
+             r=0, u=0, v=0, u_hat=(0, 0, 0), v_hat=(0, 0, 0), k_r64=0, pos64=0, out_u8=0,
+             dB_min=0.0, dB_max=0.0, precision=-1):
+    """Builds a Job from device addresses (ints, e.g. tensor.data_ptr())."""
+    j = Job()
+    j.nsamples, j.npulses, j.n_fft, j.taylor_s_l = int(nsamples), int(npulses), int(n_fft), int(taylor_s_l)
+    j.nu, j.nv, j.delta_r = int(nu), int(nv), float(delta_r)
+    j.phs, j.k_r, j.k_r64, j.pos, j.pos64 = phs or None, k_r or None, k_r64 or None, pos or None, pos64 or None
+    j.r, j.u, j.v = r or None, u or None, v or None
+    for i in range(3):
+        j.u_hat[i] = float(u_hat[i])
+        j.v_hat[i] = float(v_hat[i])
+    j.output_img, j.out_u8 = output_img or None, out_u8 or None
+    j.dB_min, j.dB_max = float(dB_min), float(dB_max)
+    j.precision = int(precision)
+    return j

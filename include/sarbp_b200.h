@@ -1,0 +1,204 @@
+/*
+ * sarbp_b200.h -- C ABI of the B200 SAR backprojection library
+ * (libsarbp_b200.so).
+ *
+ * Drop-in for the `-s cuda` path of ISI-apex/halide-sar-app: the same
+ * inputs as the reference's Halide pipeline `backprojection_cuda`
+ * (backprojection.cpp:35-46, called at sarbp.cpp:277), as plain pointers
+ * and sizes, plus the dB / u8 output stages (img_output.cpp:10-52).
+ *
+ * Conventions
+ *  - Every function returns an int status: SARBP_OK (0) or a negative
+ *    SARBP_ERR_* code; sarbp_last_error() gives a message for the calling
+ *    thread.  Nothing aborts and no kernel traps.
+ *  - Layouts follow the reference's Halide buffers:
+ *      phs        complex64 [npulses][nsamples]   (Halide {2, S, P})
+ *      k_r        [nsamples]
+ *      pos        [npulses][3]                    (Halide {3, P})
+ *      r          SoA [3][nu*nv], pixel i at u index i % nu, v index i / nu
+ *                                                 (Halide {nu*nv, 3})
+ *      output_img complex128 [nv][nu], rows flipped as in
+ *                 backprojection.cpp:130          (Halide {2, nu, nv})
+ *  - Functions named *_device take device pointers and enqueue on the
+ *    context's stream without synchronising; the others take host pointers
+ *    and return when the result is in host memory.
+ *  - A context is used by one host thread at a time.
+ */
+#ifndef SARBP_B200_H
+#define SARBP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SARBP_OK 0
+#define SARBP_ERR_INVALID (-1)     /* bad argument, shape or size */
+#define SARBP_ERR_UNSUPPORTED (-2) /* e.g. N_fft not a power of two in [16, 16384] */
+#define SARBP_ERR_NOMEM (-3)       /* device or host allocation failed */
+#define SARBP_ERR_CUDA (-4)        /* a CUDA runtime call failed */
+#define SARBP_ERR_GEOMETRY (-5)    /* non-finite geometry, or a pixel tile whose
+                                      range window does not fit on chip */
+#define SARBP_ERR_TIMEOUT (-6)     /* a bounded wait gave up */
+#define SARBP_ERR_ADMISSION (-7)   /* serving: job exceeds the HBM cap */
+#define SARBP_ERR_STATE (-8)       /* call not valid in the current state */
+
+/* Precision of the pulse-accumulation kernel. */
+#define SARBP_PREC_COMPAT 0  /* the reference's semantics: f32 pos, f32 |pos|
+                                (norm_r0), f32 k_c; split-precision kernel */
+#define SARBP_PREC_PRECISE 1 /* f64 per-pulse geometry (positions, |pos|, k_c);
+                                split-precision kernel */
+#define SARBP_PREC_NAIVE 2   /* plain FP32 range and phase per pixel*pulse
+                                (precision-study baseline) */
+
+typedef struct sarbp_ctx sarbp_ctx;
+
+/* Kernel tuning; a zero field means "library default / autotuned". */
+typedef struct sarbp_opts {
+    int precision;   /* SARBP_PREC_* */
+    int tile_x;      /* pixel tile width  (8, 16, 32 or 64) */
+    int tile_y;      /* pixel tile height (must give tile_x*tile_y in {256..4096}) */
+    int pulse_chunk; /* pulses staged per chunk (4..256) */
+    int persistent;  /* 0 or 1: persistent work-list launch; 2: one CTA per tile */
+    int stage_cap;   /* float4 entries of the range-window staging buffer */
+    int reserved[2];
+} sarbp_opts;
+
+/*
+ * One image-formation job with all arrays device-resident.  Exactly one of
+ * (r) or (u, v, u_hat, v_hat) describes the pixel positions: when r is
+ * NULL, pixel (ix, iy) sits at u_hat*u[ix] + v_hat*v[iy]
+ * (img_plane.cpp:92-102) and no nu*nv*3 position array is read.
+ */
+typedef struct sarbp_job {
+    int nsamples, npulses, n_fft, taylor_s_l, nu, nv;
+    double delta_r;
+    const float *phs;    /* complex64 [P][S] */
+    const float *k_r;    /* [S] f32, used in COMPAT / NAIVE */
+    const double *k_r64; /* [S] f64, used in PRECISE (may be NULL -> k_r) */
+    const float *pos;    /* [P][3] f32, used in COMPAT / NAIVE */
+    const double *pos64; /* [P][3] f64, used in PRECISE (may be NULL -> pos) */
+    const double *r;     /* SoA [3][nu*nv] or NULL */
+    const double *u;     /* [nu], when r == NULL */
+    const double *v;     /* [nv], when r == NULL */
+    double u_hat[3], v_hat[3];
+    double *output_img;  /* complex128 [nv][nu] (device) */
+    uint8_t *out_u8;     /* optional: u8 image [nv][nu] (device), or NULL */
+    double dB_min, dB_max; /* used when out_u8 != NULL */
+    int precision;       /* SARBP_PREC_*; overrides opts->precision when >= 0 */
+    int reserved;
+} sarbp_job;
+
+/* ---- context ---- */
+int sarbp_ctx_create(int device, sarbp_ctx **out);
+int sarbp_ctx_destroy(sarbp_ctx *ctx);
+/* Launch on a caller-owned cudaStream_t (NULL = the context's own stream). */
+int sarbp_ctx_set_stream(sarbp_ctx *ctx, void *cuda_stream);
+void *sarbp_ctx_stream(sarbp_ctx *ctx);
+int sarbp_ctx_synchronize(sarbp_ctx *ctx);
+/* Kernels this context has launched so far (all entry points). */
+long long sarbp_ctx_launch_count(sarbp_ctx *ctx);
+/* Record CUDA events around each stage of every batch (on = 1). */
+int sarbp_ctx_set_timing(sarbp_ctx *ctx, int on);
+/* Device time (ms) of the last batch's stages: [0] set-up kernel, [1] range
+ * compression, [2] backprojection, [3] u8 output; -1 for a stage that did
+ * not run.  Waits for the batch. */
+int sarbp_ctx_last_stage_ms(sarbp_ctx *ctx, float *ms4);
+/* Measured FP32 FFMA instructions/s and SFU (MUFU) operations/s of the
+ * context's device, from two chain microkernels. */
+int sarbp_measure_peaks(sarbp_ctx *ctx, double *ffma_per_s, double *mufu_per_s);
+const char *sarbp_last_error(void);
+const char *sarbp_version(void);
+
+/*
+ * Backprojection with host buffers: replaces the Halide pipeline
+ * `int backprojection_cuda(phs, k_r, taylor_s_l, N_fft, delta_r, u, v, pos,
+ * r, output_img)` (backprojection.cpp:35-46, sarbp.cpp:277).  Range
+ * compression (the FFTW extern call_dft, dft.cpp:40-79) runs on the device.
+ * opts may be NULL (SARBP_PREC_COMPAT, autotuned tiles).
+ */
+int sarbp_backprojection(sarbp_ctx *ctx, const float *phs, int nsamples,
+                         int npulses, const float *k_r, int taylor_s_l,
+                         int n_fft, double delta_r, const double *u, int nu,
+                         const double *v, int nv, const float *pos,
+                         const double *r, double *output_img,
+                         const sarbp_opts *opts);
+
+/* The same with f64 positions and k_r (SARBP_PREC_PRECISE by default). */
+int sarbp_backprojection_f64(sarbp_ctx *ctx, const float *phs, int nsamples,
+                             int npulses, const double *k_r, int taylor_s_l,
+                             int n_fft, double delta_r, const double *u,
+                             int nu, const double *v, int nv,
+                             const double *pos, const double *r,
+                             double *output_img, const sarbp_opts *opts);
+
+/* Device-resident single job (enqueued, not synchronised). */
+int sarbp_backprojection_device(sarbp_ctx *ctx, const sarbp_job *job,
+                                const sarbp_opts *opts);
+
+/*
+ * Range compression only (backprojection.cpp:79-104 with the FFT extern
+ * call_dft, dft.cpp:40-79): writes the complex64 range profiles Q
+ * [npulses][n_fft] of `job` to the device buffer q_out.  The pixel and
+ * output fields of `job` are not used.
+ */
+int sarbp_range_compress_device(sarbp_ctx *ctx, const sarbp_job *job,
+                                const sarbp_opts *opts, float *q_out);
+
+/*
+ * Many jobs of uneven size in one batch: one window kernel, one range
+ * compression launch per distinct N_fft, and one persistent backprojection
+ * launch over a (job, pixel tile) work list ordered longest-first.
+ * Enqueued on the context's stream, not synchronised.
+ */
+int sarbp_batch_device(sarbp_ctx *ctx, const sarbp_job *jobs, int njobs,
+                       const sarbp_opts *opts);
+
+/* ---- dB / u8 output stages (img_output.cpp:10-52) ---- */
+/* dB = 10*log10(|z| / max|z|) for a complex128 [nv][nu] image. */
+int sarbp_img_output_to_dB(sarbp_ctx *ctx, const double *img, int nu, int nv,
+                           double *dB);
+/* u8 = trunc(clamp((clamp(dB,min,max)-min)/(max-min)*255, 0, 255)). */
+int sarbp_img_output_u8(sarbp_ctx *ctx, const double *dB, int nu, int nv,
+                        double dB_min, double dB_max, uint8_t *out);
+int sarbp_img_output_to_dB_device(sarbp_ctx *ctx, const double *img, int nu,
+                                  int nv, double *dB);
+int sarbp_img_output_u8_device(sarbp_ctx *ctx, const double *dB, int nu,
+                               int nv, double dB_min, double dB_max,
+                               uint8_t *out);
+
+/* ---- host helpers used by the CLI and the harness ---- */
+/* Taylor window (signal.h:14-51), f64 [num]. */
+int sarbp_taylor(int num, double S_L, double *out);
+/* nu/nv of img_plane_create (ImgPlane.cpp:20-28). */
+int sarbp_img_plane_dims(int nsamples, int npulses, int upsample, int *nu,
+                         int *nv);
+/* img_plane_create (ImgPlane.cpp:16-63): u[nu], v[nv], k_u, k_v, u_hat[3],
+ * v_hat[3], and pixel_locs SoA [3][nu*nv] when non-NULL. */
+int sarbp_img_plane(int nsamples, int npulses, double delta_r,
+                    const float *R_c, const float *n_hat, double res_factor,
+                    double aspect, int upsample, double *d_u, double *d_v,
+                    double *u, double *v, double *k_u, double *k_v,
+                    double *u_hat, double *v_hat, double *pixel_locs);
+
+/*
+ * Seeded synthetic stepped-frequency phase history (the harness's stand-in
+ * for the AFRL / Sandia data): circular aperture of npulses positions at
+ * slant range R0, depression dep_deg, azimuth span span_deg, centred on the
+ * scene origin; scatterers (x, y, z, amplitude re, im) summed as
+ * S(f,p) = sum_i a_i exp(+j 4 pi f/c (|p| - |p - x_i|)), plus complex
+ * Gaussian noise at snr_db (no noise when snr_db >= 300).
+ * Outputs: phs complex64 [P][S], pos f64 [P][3], k_r f64 [S].
+ */
+int sarbp_synth_phase_history(int nsamples, int npulses, double f0, double df,
+                              double R0, double dep_deg, double span_deg,
+                              const double *scat, int nscat, double snr_db,
+                              uint64_t seed, float *phs, double *pos,
+                              double *k_r, int nthreads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,107 @@
+"""The C ABI library: loads, exports every declared symbol, host helpers
+(CPU only; no kernel is launched here)."""
+import ctypes
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def _declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        if 'extern "C"' not in src:
+            continue
+        for m in re.finditer(r"\b(sarbp_\w+)\s*\(", src):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_symbol(sb):
+    from sarbp_b200 import _lib
+    L = _lib.lib()
+    declared = _declared_functions()
+    assert len(declared) >= 15
+    missing = [n for n in declared if not hasattr(L, n)]
+    assert not missing, missing
+    # and the Python binding covers all of them
+    assert declared <= set(_lib.SIGNATURES), declared - set(_lib.SIGNATURES)
+
+
+def test_version(sb):
+    assert "sm_100a" in sb.version()
+
+
+def test_taylor_matches_oracle(sb, oracle, known_answers):
+    ka = known_answers["taylor"]
+    np.testing.assert_array_equal(sb.taylor(ka["num"], ka["S_L"]), oracle.taylor(ka["num"], ka["S_L"]))
+    for n, sl in ((1999, 30), (424, 17), (1024, 20)):
+        np.testing.assert_array_equal(sb.taylor(n, sl), oracle.taylor(n, sl))
+
+
+def test_img_plane_matches_fixture(sb, afrl_input, afrl_img_plane):
+    ip = sb.img_plane_create(int(afrl_input["nsamples"][0]), int(afrl_input["npulses"][0]),
+                             float(afrl_input["delta_r"][0]), afrl_input["R_c"])
+    for k in ("u", "v", "k_u", "k_v"):
+        np.testing.assert_array_equal(ip[k], afrl_img_plane[k])
+    np.testing.assert_allclose(ip["v_hat"], afrl_img_plane["v_hat"], atol=1e-7, rtol=0)
+    assert ip["pixel_locs"].shape == (3, 512 * 512)
+
+
+def test_img_plane_and_pixel_locs_match_oracle(sb, oracle):
+    R_c = np.array([1234.5, -3000.25, 4000.0], np.float32)
+    for up in (True, False):
+        a = sb.img_plane_create(300, 129, 0.3, R_c, res_factor=0.7, aspect=1.3, upsample=up)
+        b = oracle.img_plane(300, 129, 0.3, R_c, res_factor=0.7, aspect=1.3, upsample=up)
+        for k in ("u", "v", "k_u", "k_v", "u_hat", "v_hat", "pixel_locs"):
+            np.testing.assert_array_equal(a[k], b[k])
+        np.testing.assert_array_equal(sb.pixel_locs(a["u"], a["v"], a["u_hat"], a["v_hat"]),
+                                      b["pixel_locs"])
+
+
+def test_n_fft_rule(sb):
+    # sarbp.cpp:258
+    assert sb.n_fft_for(424, 2) == 1024
+    assert sb.n_fft_for(1024, 2) == 4096
+    assert sb.n_fft_for(2048, 2) == 8192
+    assert sb.n_fft_for(424, 6) == 4096
+    assert sb.n_fft_for(1800, 6) == 16384
+
+
+def test_synth_deterministic_and_threads_independent(sb):
+    from sarbp_b200 import synth
+    scat = synth.scene(5, 10.0, 3, seed=4)
+    a = synth.phase_history(64, 33, 9.3e9, 1.5e6, 10e3, 30, 4, scat, 20.0, 11, nthreads=1)
+    b = synth.phase_history(64, 33, 9.3e9, 1.5e6, 10e3, 30, 4, scat, 20.0, 11, nthreads=5)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+    phs, pos, k_r = a
+    assert phs.dtype == np.complex64 and phs.shape == (33, 64)
+    np.testing.assert_allclose(np.linalg.norm(pos, axis=1), 10e3, rtol=1e-12)
+
+
+def test_synth_matches_direct_sum(sb):
+    from sarbp_b200 import synth
+    scat = np.array([[1.0, 2.0, 0.0, 0.7, -0.2], [-3.0, 0.5, 0.0, 0.1, 0.4]])
+    phs, pos, k_r = synth.phase_history(100, 7, 9.3e9, 1.5e6, 10e3, 30, 4, scat, 400, 1)
+    D = np.linalg.norm(pos, axis=1)[:, None] - np.linalg.norm(pos[:, None, :] - scat[None, :, :3], axis=2)
+    a = scat[:, 3] + 1j * scat[:, 4]
+    ref = (a[None, None, :] * np.exp(1j * k_r[None, :, None] * D[:, None, :])).sum(-1)
+    np.testing.assert_allclose(phs, ref, rtol=0, atol=2e-6)
+
+
+def test_errors_without_gpu_are_codes(sb):
+    """Creating a context on a machine without a usable B200 returns an
+    error code and a message instead of crashing."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(sb.SarbpError) as ei:
+        sb.Context(0)
+    assert ei.value.code in (sb._lib.ERR_CUDA, sb._lib.ERR_INVALID)
