@@ -43,7 +43,7 @@ SFU_PER_UNIT = 3    # SFU operations per pixel*pulse (algorithmic)
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="plain_large")
@@ -51,8 +51,11 @@ def parse():
                     help="CPU work of the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer timing (profiling)")
     ap.add_argument("--tile", default="", help="e.g. 32x32")
     ap.add_argument("--chunk", type=int, default=0)
+    ap.add_argument("--stage-cap", type=int, default=0)
+    ap.add_argument("--min-blocks", type=int, default=0)
     return ap.parse_args()
 
 
@@ -239,6 +242,10 @@ def run_ours(args, rank, world, local_rank):
         tune["tile"] = tuple(int(x) for x in args.tile.split("x"))
     if args.chunk:
         tune["pulse_chunk"] = args.chunk
+    if args.stage_cap:
+        tune["stage_cap"] = args.stage_cap
+    if args.min_blocks:
+        tune["min_blocks"] = args.min_blocks
     job = sb.make_job(S, P, data["N_fft"], data["taylor"], nu, nv, data["delta_r"], t_phs.data_ptr(),
                       t_k.data_ptr(), t_pos.data_ptr(), t_out.data_ptr(), r=t_r.data_ptr())
 
@@ -285,7 +292,7 @@ def run_ours(args, rank, world, local_rank):
     u8_ms = []
     for _ in range(3):
         ctx.run_jobs([job_u8], **tune)
-        u8_ms.append(ctx.last_stage_ms()[3])
+        u8_ms.append(ctx.last_stage_ms()[4])
     ctx.synchronize()
 
     # ---- e2e through the host-buffer entry point, pinned host memory ----
@@ -305,7 +312,10 @@ def run_ours(args, rank, world, local_rank):
             ctx.handle, p(h_phs), S, P, p(h_k), data["taylor"], data["N_fft"], data["delta_r"], p(h_u),
             nu, p(h_v), nv, p(h_pos), p(h_r), p(out_pinned), ctypes.byref(o)))
 
-    e2e_call()
+    if args.no_e2e:
+        args.e2e_steps = 0
+    else:
+        e2e_call()
     barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -314,18 +324,19 @@ def run_ours(args, rank, world, local_rank):
         e2e_call()
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
+    e2e_ms = max(e0.elapsed_time(e1), 1e-6)
     if world > 1:
         t = torch.tensor([e2e_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    e2e_value = world * units * args.e2e_steps / (e2e_ms * 1e-3) / 1e9
+    e2e_value = world * units * args.e2e_steps / (e2e_ms * 1e-3) / 1e9 if args.e2e_steps else None
     h2d = h_phs.nbytes + h_k.nbytes + h_pos.nbytes + h_r.nbytes
     d2h = out_pinned.nbytes
 
     # ---- roofline of the backprojection kernel (FP32 + SFU) ----
     st = np.array(stage)
-    bp_ms = float(st[:, 2].mean())
+    bp_ms = float(st[:, 3].mean())
+    geom_ms = float(st[:, 2].mean())
     rc_ms = float(st[:, 1].mean())
     prep_ms = float(st[:, 0].mean())
     bp_units_s = units / (bp_ms * 1e-3)
@@ -353,7 +364,7 @@ def run_ours(args, rank, world, local_rank):
         "data": "synthetic (seeded, plain_large shapes)",
         "config": config_block(data, world),
         "gpu_launches": int(launches),
-        "stage_ms": {"setup": prep_ms, "range_compress": rc_ms, "backproject": bp_ms,
+        "stage_ms": {"setup": prep_ms, "range_compress": rc_ms, "tile_geometry": geom_ms, "backproject": bp_ms,
                      "db_u8": float(np.mean(u8_ms))},
         "roofline": {"bound": bound, "achieved": achieved, "peak": peak, "unit": "Tops/s",
                      "frac": achieved / peak, "traffic": None,
@@ -374,7 +385,7 @@ def run_ours(args, rank, world, local_rank):
                       "frac": u8_bytes / (np.mean(u8_ms) * 1e-3) / 1e9 / hbm_peak, "bytes": u8_bytes},
             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s"},
         "e2e": {"value": e2e_value, "unit": "Gpixel*pulses/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms / args.e2e_steps,
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms / max(args.e2e_steps, 1),
                 "steps": args.e2e_steps},
         "clocks": clk,
     }

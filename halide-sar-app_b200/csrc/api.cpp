@@ -188,21 +188,22 @@ int sarbp_ctx_set_timing(sarbp_ctx *ctx, int on) {
     return SARBP_OK;
 }
 
-int sarbp_ctx_last_stage_ms(sarbp_ctx *ctx, float *ms4) {
+int sarbp_ctx_last_stage_ms(sarbp_ctx *ctx, float *ms5) {
     int rc = set_device(ctx);
     if (rc) return rc;
-    if (!ms4) return fail(SARBP_ERR_INVALID, "ms4 is NULL");
+    if (!ms5) return fail(SARBP_ERR_INVALID, "ms5 is NULL");
     DeviceInfo &d = ctx->dev;
-    for (int i = 0; i < 4; ++i) ms4[i] = -1.0f;
+    constexpr int kStages = DeviceInfo::kEvents - 1;
+    for (int i = 0; i < kStages; ++i) ms5[i] = -1.0f;
     if (!d.ev_recorded[0]) return fail(SARBP_ERR_STATE, "no timed batch (enable sarbp_ctx_set_timing)");
-    for (int i = 0; i < 5; ++i)
+    for (int i = 0; i < DeviceInfo::kEvents; ++i)
         if (d.ev_recorded[i]) {
             cudaError_t e = cudaEventSynchronize(d.ev[i]);
             if (e != cudaSuccess) return cuda_fail(e, "cudaEventSynchronize");
         }
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < kStages; ++i)
         if (d.ev_recorded[i] && d.ev_recorded[i + 1]) {
-            cudaError_t e = cudaEventElapsedTime(&ms4[i], d.ev[i], d.ev[i + 1]);
+            cudaError_t e = cudaEventElapsedTime(&ms5[i], d.ev[i], d.ev[i + 1]);
             if (e != cudaSuccess) return cuda_fail(e, "cudaEventElapsedTime");
         }
     return SARBP_OK;

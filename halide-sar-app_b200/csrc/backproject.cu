@@ -2,28 +2,36 @@
 //
 // Split-precision tile kernel
 // ---------------------------
-// One CTA forms one pixel tile (TX x TY pixels, NT threads, PPT pixels per
-// thread).  The tile centre r_c and radius rho are found once.  For every
-// (tile, pulse) the large terms are evaluated once in f64:
-//     w    = pos_p - r_c,  R = |w|,  dr_c = |pos_p| - R
-//     t_c  = (dr_c - lsa) / lsr        (range-bin coordinate of the centre)
-//     B    = exp(-j k_c dr_c)          (phase reduced in f64, then sincospi)
-// and only the small offset of a pixel, delta = r - r_c (|delta| <= rho, a
-// metre or two), goes through FP32 per pixel*pulse:
-//     h     = w_hat . delta - |delta|^2 / (2R)
-//     Delta = h (1 + g [+ 2 g^2]),  g = h / (2R)   = R - |w - delta|
-//     dr    = dr_c + Delta
-// (a series of R - sqrt(R^2 - 2Rh); a chunk whose pulses are too close for
-// the series to meet the phase tolerance switches to the closed form
-// 2Rh / (R + sqrt(R (R - 2h)))).  Delta is at most rho, so each pulse only
-// touches a window of W = 2K+1 range bins around floor(t_c); the window is
-// staged in shared memory per pulse chunk as
-//     (m, d) = ((Q[k] + Q[k+1]) / 2, Q[k+1] - Q[k]) * B
-// so the reference's clamped lerp Q[l](1-w) + Q[l+1]w becomes m + (w-1/2) d
-// (one 16-byte shared load), and the carrier left per pixel is
-// exp(-j k_c Delta), a few hundred radians at most, evaluated with the SFU.
-// The bin index comes from the float itself (add 1.5*2^23 and read the low
-// mantissa bits), which keeps the floor off the conversion pipe.
+// One CTA forms one pixel tile (TX x TY pixels).  All f64 geometry was done
+// ahead of it (geometry.cu): the tile centre rc, radius rho, window
+// half-width K, the final phase per pixel, and per (tile, pulse) a record
+// with w_hat = (pos - rc)/R, e = 1/(2 k_c R), the base bin, and the phase
+// theta = k_c dr_c reduced to [-pi, pi).  Only the small offset of a pixel,
+// d = k_c (r - rc) (|r - rc| <= rho, a metre or two), goes through FP32 per
+// pixel*pulse, in radians:
+//     s     = w_hat . d,   t = s^2 - |d|^2
+//     Delta = s + e t     (= k_c (R - |pos - r|) up to k_c rho^3/(2R^2))
+//     phase = theta + Delta,  range bin = t_c + Delta / (k_c lsr)
+// A chunk whose pulses are close enough for that truncation to exceed the
+// phase budget adds the next term, s + e t (1 + 2 e s); closer still, the
+// closed form 2R'h / (R' + sqrt(R'(R' - 2h))), R' = k_c R, h = s - e|d|^2,
+// is used.  |Delta| <= k_c rho, so each pulse only touches W = 2K+1 range
+// bins; range compression stored every bin as the pair
+//     (m, d) = ((Q[k] + Q[k+1]) / 2, Q[k+1] - Q[k])
+// so the reference's clamped lerp Q[l](1-w) + Q[l+1]w is m + (w-1/2) d: one
+// 16-byte shared load.  The bin index is read from the float itself (add
+// 1.5*2^23; the low mantissa bits are the integer) and one shift-add turns
+// it into the staging address.
+//
+// Warp roles: 8 consumer warps own the pixels (PPT per thread) and run only
+// the accumulation loop.  One producer warp stages chunk c into half b = c&1
+// of a double buffer: a bulk asynchronous copy of the chunk's pulse records,
+// then one bulk copy per pulse of its W-entry window of (m, d) pairs (window
+// parts outside the profile are filled with the clamped edge pair), both
+// completing on mbarriers with bounded waits.  Hand-over uses named
+// barriers: FULL[b] producer -> consumers, EMPTY[b] consumers -> producer;
+// each instance gets one arrival set from each side, and the producer
+// drains the last two EMPTY instances of every tile.
 //
 // Work list: items are (job, tile); with `persistent` the grid is the number
 // of resident CTAs and each CTA pulls items (ordered longest first by the
@@ -32,6 +40,7 @@
 // Naive kernel: the same quantity with plain FP32 range |pos| - |r - pos|
 // and phase k_c * dr per pixel*pulse; kept as the precision-study baseline.
 #include <cfloat>
+#include <cstdint>
 
 #include "internal.h"
 #include "kernels.h"
@@ -40,298 +49,317 @@ namespace sarbp {
 
 namespace {
 
-constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
-constexpr int kMagicBits = 0x4B400000;
-constexpr int kNT = 256;               // threads per CTA
-constexpr double kInv2Pi = 0.15915494309189533577;
-constexpr float kPhaseTol = 2e-5f;     // rad, truncation budget of the series
+constexpr float kMagic = 12582912.0f;             // 1.5 * 2^23
+constexpr uint32_t kMagicBits = 0x4B400000u;
+constexpr uint32_t kMagicOff = kMagicBits << 4;   // (mod 2^32) byte offset of index 0
+constexpr int kConsumers = 256;                   // consumer threads (8 warps)
+constexpr int kConsumerWarps = kConsumers / 32;
+constexpr int kThreads = kConsumers + 32;         // plus one producer warp
+constexpr int kBarFull0 = 1;                      // named barriers 1, 2: chunk staged
+constexpr int kBarEmpty0 = 3;                     // named barriers 3, 4: chunk consumed
 
-struct __align__(16) PulseA {
-    float wx, wy, wz, e;  // w_hat, 1/(2R)
-};
-struct __align__(16) PulseB {
-    float c0;    // t_c - floor(t_c) + K - 1/2
-    float R;     // |w|
-    int off;     // offset of the pulse's window in the staging buffer
-    int pad;
-};
-
-__device__ __forceinline__ double warp_min(double v) {
-    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
+__device__ __forceinline__ void bar_sync(int id) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(kThreads) : "memory");
+}
+__device__ __forceinline__ void bar_arrive(int id) {
+    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(kThreads) : "memory");
+}
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
 }
 __device__ __forceinline__ double warp_max(double v) {
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
 }
 
-// Inner loop over the nc pulses of a chunk for the thread's PPT pixels.
-// MODE 0: Delta = h(1+g); 1: Delta = h(1+g+2g^2); 2: closed form.
-template <int MODE, int PPT>
-__device__ __forceinline__ void accumulate(int nc, const PulseA *__restrict__ pa,
-                                           const PulseB *__restrict__ pb,
-                                           const float4 *__restrict__ stage, float inv_lsr,
-                                           float kc, float hi_clamp, const float (&dx)[PPT],
-                                           const float (&dy)[PPT], const float (&dz)[PPT],
-                                           const float (&nd2)[PPT], float (&ar)[PPT],
+// Bounded wait on an mbarrier phase; false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    for (int it = 0; it < (1 << 22); ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void mbar_expect(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_copy(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Inner loop over the nc pulses of a chunk for a consumer's PPT pixels.
+// MODE 0: Delta = s + e t; 1: s + e t (1 + 2 e s); 2: closed form.
+// PLANAR: every pixel of the tile has dz == 0.
+template <int MODE, bool PLANAR, int PPT>
+__device__ __forceinline__ void accumulate(int nc, const PulseRec *__restrict__ rec, uint32_t poff,
+                                           uint32_t pstride, float ilk, float hi_clamp,
+                                           const float (&dx)[PPT], const float (&dy)[PPT],
+                                           const float (&dz)[PPT], const float (&nd2)[PPT], float (&ar)[PPT],
                                            float (&ai)[PPT]) {
 #pragma unroll 2
-    for (int i = 0; i < nc; ++i) {
-        const PulseA a = pa[i];
-        const PulseB b = pb[i];
-        const float4 *__restrict__ st = stage + b.off;
+    for (int i = 0; i < nc; ++i, poff += pstride) {
+        const float4 a = rec[i].a;  // w_hat, e
+        const float4 b = rec[i].b;  // c0, theta, R', bits
+        const float e2 = a.w + a.w;
 #pragma unroll
         for (int k = 0; k < PPT; ++k) {
-            float h = fmaf(a.wx, dx[k], fmaf(a.wy, dy[k], fmaf(a.wz, dz[k], nd2[k] * a.e)));
+            float s = fmaf(a.y, dy[k], a.x * dx[k]);
+            if constexpr (!PLANAR) s = fmaf(a.z, dz[k], s);
             float D;
             if constexpr (MODE == 0) {
-                const float g = h * a.e;
-                D = fmaf(h, g, h);
+                D = fmaf(a.w, fmaf(s, s, nd2[k]), s) + b.y;
             } else if constexpr (MODE == 1) {
-                const float g = h * a.e;
-                D = fmaf(h * g, fmaf(2.0f, g, 1.0f), h);
+                const float t = fmaf(s, s, nd2[k]);
+                D = fmaf(a.w * t, fmaf(e2, s, 1.0f), s) + b.y;
             } else {
-                // 2Rh / (R + sqrt(R (R - 2h)))
-                const float q = fmaxf(fmaf(-2.0f, h, b.R), 0.0f);
-                const float s = sqrtf(b.R * q);
-                D = (2.0f * b.R * h) / (b.R + s);
+                const float h = fmaf(a.w, nd2[k], s);
+                const float q = fmaxf(fmaf(-2.0f, h, b.z), 0.0f);
+                const float r = sqrtf(b.z * q);
+                D = (2.0f * b.z * h) / (b.z + r) + b.y;
             }
-            float tl = fmaf(D, inv_lsr, b.c0);
+            float tl = fmaf(D, ilk, b.x);
             if constexpr (MODE == 2) tl = fminf(fmaxf(tl, 0.0f), hi_clamp);
             const float f = tl + kMagic;
             const float wgt = tl - (f - kMagic);
-            const int j = __float_as_int(f) - kMagicBits;
-            const float4 md = st[j];
+            const uint32_t o = (__float_as_uint(f) << 4) + poff;  // shared-window address
+            float4 md;
+            asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                         : "=f"(md.x), "=f"(md.y), "=f"(md.z), "=f"(md.w)
+                         : "r"(o));
             const float vr = fmaf(wgt, md.z, md.x);
             const float vi = fmaf(wgt, md.w, md.y);
-            float s, c;
-            __sincosf(D * kc, &s, &c);
-            ar[k] = fmaf(vr, c, fmaf(vi, s, ar[k]));
-            ai[k] = fmaf(vi, c, fmaf(-vr, s, ai[k]));
+            float sn, cs;
+            __sincosf(D, &sn, &cs);
+            ar[k] = fmaf(vr, cs, fmaf(vi, sn, ar[k]));
+            ai[k] = fmaf(vi, cs, fmaf(-vr, sn, ai[k]));
         }
     }
 }
 
-template <int TX, int TY>
-__global__ void __launch_bounds__(kNT) bp_tile_kernel(const DevJob *__restrict__ jobs,
-                                                      const WorkItem *__restrict__ items, int nitems,
-                                                      int *__restrict__ counter, int stage_cap,
-                                                      int cmax, int persistent) {
-    constexpr int PPT = TX * TY / kNT;
-    constexpr int ROWS = kNT / TX;
-    static_assert(PPT >= 1 && TX * TY == PPT * kNT, "tile must be a multiple of the CTA");
-    extern __shared__ float4 smem[];
-    float4 *stage = smem;
-    PulseA *pa = reinterpret_cast<PulseA *>(stage + stage_cap);
-    PulseB *pb = reinterpret_cast<PulseB *>(pa + cmax);
-    float2 *pB = reinterpret_cast<float2 *>(pb + cmax);
-    int *pbase = reinterpret_cast<int *>(pB + cmax);
-    float2 *fin = reinterpret_cast<float2 *>(pbase + cmax);  // [TX*TY]
-    __shared__ double sred[6][kNT / 32];
-    __shared__ float sredf[kNT / 32];
-    __shared__ int s_item;
+template <int PPT>
+__device__ __forceinline__ void accumulate_any(int mode, bool planar, int nc, const PulseRec *rec,
+                                               uint32_t poff, uint32_t pstride, float ilk, float hi,
+                                               const float (&dx)[PPT], const float (&dy)[PPT],
+                                               const float (&dz)[PPT], const float (&nd2)[PPT],
+                                               float (&ar)[PPT], float (&ai)[PPT]) {
+    if (mode == 0) {
+        if (planar) accumulate<0, true, PPT>(nc, rec, poff, pstride, ilk, hi, dx, dy, dz, nd2, ar, ai);
+        else accumulate<0, false, PPT>(nc, rec, poff, pstride, ilk, hi, dx, dy, dz, nd2, ar, ai);
+    } else if (mode == 1) {
+        if (planar) accumulate<1, true, PPT>(nc, rec, poff, pstride, ilk, hi, dx, dy, dz, nd2, ar, ai);
+        else accumulate<1, false, PPT>(nc, rec, poff, pstride, ilk, hi, dx, dy, dz, nd2, ar, ai);
+    } else {
+        accumulate<2, false, PPT>(nc, rec, poff, pstride, ilk, hi, dx, dy, dz, nd2, ar, ai);
+    }
+}
 
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int lx = tid % TX, ly = tid / TX;
+// Shared memory of the tile kernel.
+struct TileSmem {
+    float4 *stage;       // [2][stage_cap] (m, d) windows
+    PulseRec *rec;       // [2][cmax]
+    uint64_t *mbar_rec;  // [2]
+    uint64_t *mbar_win;  // [2]
+    double *sred;        // [kConsumerWarps]
+    int *s_item, *s_mode;
+};
 
+struct TileShape {
+    int K, W, C, nchunks;
+};
+
+__device__ __forceinline__ TileShape tile_shape(const TileInfo &t, int P, int stage_cap, int cmax) {
+    TileShape s;
+    s.K = t.K;
+    s.W = 2 * t.K + 1;
+    int C = stage_cap / s.W;
+    if (C > cmax) C = cmax;
+    if (C > P) C = P;
+    s.C = C;
+    s.nchunks = C >= 1 ? (P + C - 1) / C : 0;
+    return s;
+}
+
+// Producer warp, one chunk into half b: records, then windows.
+__device__ __forceinline__ bool stage_chunk(const DevJob &jb, int tile, int lane, int p0, int nc, int b,
+                                            const TileShape &sh, int stage_cap, int cmax,
+                                            const TileSmem &sm, uint32_t (&uses)[4]) {
+    const int N = jb.N, W = sh.W;
+    PulseRec *rec = sm.rec + b * cmax;
+    float4 *win = sm.stage + b * stage_cap;
+    // prior generic-proxy reads of these buffers come before the async writes
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (lane == 0) {
+        mbar_expect(&sm.mbar_rec[b], (uint32_t)(nc * (int)sizeof(PulseRec)));
+        bulk_copy(rec, jb.recs + (size_t)tile * jb.P + p0, (uint32_t)(nc * (int)sizeof(PulseRec)),
+                  &sm.mbar_rec[b]);
+    }
+    bool ok = mbar_wait(&sm.mbar_rec[b], uses[b] & 1u);
+    uses[b]++;
+    // window copies: bins [base, base + W) of row p; the in-profile part
+    // [max(base, 0), min(base + W, N)) comes from the pairs row
+    uint32_t bytes = 0;
+    int mode = 0;
+    for (int i = lane; i < nc; i += 32) {
+        const int bits = __float_as_int(rec[i].b.w);
+        const int base = bits >> 2, order = bits & 3;
+        if (order == 3) continue;  // invalid pulse: window stays zero
+        mode = max(mode, order);
+        const int lo = max(base, 0), hi = min(base + W, N);
+        if (hi > lo) bytes += (uint32_t)(hi - lo) * 16u;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+        mode = max(mode, __shfl_xor_sync(0xffffffffu, mode, o));
+    }
+    if (lane == 0) {
+        sm.s_mode[b] = mode;
+        mbar_expect(&sm.mbar_win[b], bytes);  // the arrival of this phase
+    }
+    __syncwarp();
+    for (int i = lane; i < nc; i += 32) {
+        const int bits = __float_as_int(rec[i].b.w);
+        const int base = bits >> 2, order = bits & 3;
+        const float4 *row = jb.Qp + (size_t)(p0 + i) * (N + 1);
+        float4 *dst = win + i * W;
+        if (order == 3) {
+            for (int j = 0; j < W; ++j) dst[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+            continue;
+        }
+        const int lo = max(base, 0), hi = min(base + W, N);
+        if (hi > lo) bulk_copy(dst + (lo - base), row + lo, (uint32_t)(hi - lo) * 16u, &sm.mbar_win[b]);
+        // bins < 0 read Q[0] twice, bins >= N-1 read Q[N-1] twice (clamp)
+        for (int j = 0; j < W && base + j < 0; ++j) dst[j] = row[N];
+        for (int j = max(N - base, 0); j < W; ++j) dst[j] = row[N - 1];
+    }
+    ok = mbar_wait(&sm.mbar_win[b], uses[2 + b] & 1u) && ok;
+    uses[2 + b]++;
+    return ok;
+}
+
+// Producer warp: the same barrier sequence as the consumers.
+__device__ __forceinline__ void producer_loop(const DevJob *__restrict__ jobs,
+                                              const WorkItem *__restrict__ items, int nitems,
+                                              int stage_cap, int cmax, int persistent, const TileSmem &sm) {
+    const int lane = threadIdx.x & 31;
+    // completed phases of each mbarrier: records [0..1], windows [2..3]
+    uint32_t uses[4] = {0u, 0u, 0u, 0u};
     int item = blockIdx.x;
     for (;;) {
         if (persistent) {
-            if (tid == 0) s_item = atomicAdd(counter, 1);
-            __syncthreads();
-            item = s_item;
-            __syncthreads();
+            __syncthreads();  // s_item written
+            item = *sm.s_item;
         }
         if (item >= nitems) break;
         const WorkItem wi = items[item];
         const DevJob &jb = jobs[wi.job];
-        const int nu = jb.nu, nv = jb.nv, P = jb.P, N = jb.N;
-        const long long npix = (long long)nu * nv;
+        const TileShape sh = tile_shape(jb.tiles[wi.tile], jb.P, stage_cap, cmax);
+        bool ok = true;
+        for (int c = 0; c < sh.nchunks; ++c) {
+            const int b = c & 1;
+            if (c >= 2) bar_sync(kBarEmpty0 + b);  // consumers are done with chunk c-2
+            const int p0 = c * sh.C;
+            ok = stage_chunk(jb, wi.tile, lane, p0, min(sh.C, jb.P - p0), b, sh, stage_cap, cmax, sm, uses) &&
+                 ok;
+            bar_arrive(kBarFull0 + b);
+        }
+        for (int c = sh.nchunks > 2 ? sh.nchunks - 2 : 0; c < sh.nchunks; ++c) bar_sync(kBarEmpty0 + (c & 1));
+        if (!ok && lane == 0) atomicOr(&jb.sc->status, kStatusTimeout);
+        __syncthreads();  // epilogue partials
+        if (!persistent) break;
+    }
+}
+
+template <int TX, int TY>
+__device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
+                                              const WorkItem *__restrict__ items, int nitems,
+                                              int *__restrict__ counter, int stage_cap, int cmax,
+                                              int persistent, const TileSmem &sm) {
+    constexpr int PPT = TX * TY / kConsumers;
+    constexpr int ROWS = kConsumers / TX;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int lx = tid % TX, ly = tid / TX;
+    const uint32_t stage_base = smem_u32(sm.stage) - kMagicOff;
+    int item = blockIdx.x;
+    for (;;) {
+        if (persistent) {
+            if (tid == 0) *sm.s_item = atomicAdd(counter, 1);
+            __syncthreads();
+            item = *sm.s_item;
+        }
+        if (item >= nitems) break;
+        const WorkItem wi = items[item];
+        const DevJob &jb = jobs[wi.job];
+        const int nu = jb.nu, nv = jb.nv, P = jb.P;
         const int tx0 = (wi.tile % jb.tiles_x) * TX;
         const int ty0 = (wi.tile / jb.tiles_x) * TY;
+        const TileInfo ti = jb.tiles[wi.tile];
+        const TileShape sh = tile_shape(ti, P, stage_cap, cmax);
+        const double k_c = jb.sc->k_c;
+        const float kcf = (float)k_c;
 
-        // ---- pixel positions (f64) and the tile's bounding box ----
-        double prx[PPT], pry[PPT], prz[PPT];
-        bool act[PPT];
-        double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
-        bool bad = false;
+        // ---- pixel offsets from the tile centre, in radians ----
+        float dx[PPT], dy[PPT], dz[PPT], nd2[PPT], ar[PPT], ai[PPT];
 #pragma unroll
         for (int k = 0; k < PPT; ++k) {
             const int ix = tx0 + lx, iy = ty0 + ly + k * ROWS;
-            act[k] = ix < nu && iy < nv;
-            prx[k] = pry[k] = prz[k] = 0.0;
-            if (act[k]) {
+            dx[k] = dy[k] = dz[k] = nd2[k] = ar[k] = ai[k] = 0.0f;
+            if (ix < nu && iy < nv) {
+                double x, y, z;
                 if (jb.r) {
+                    const long long npix = (long long)nu * nv;
                     const long long pix = (long long)iy * nu + ix;
-                    prx[k] = jb.r[pix];
-                    pry[k] = jb.r[npix + pix];
-                    prz[k] = jb.r[2 * npix + pix];
+                    x = jb.r[pix];
+                    y = jb.r[npix + pix];
+                    z = jb.r[2 * npix + pix];
                 } else {
                     // img_plane.cpp:92-102: (0 + u_hat*u) + v_hat*v
                     const double uu = jb.u[ix], vv = jb.v[iy];
-                    prx[k] = __dadd_rn(__dmul_rn(jb.uh[0], uu), __dmul_rn(jb.vh[0], vv));
-                    pry[k] = __dadd_rn(__dmul_rn(jb.uh[1], uu), __dmul_rn(jb.vh[1], vv));
-                    prz[k] = __dadd_rn(__dmul_rn(jb.uh[2], uu), __dmul_rn(jb.vh[2], vv));
+                    x = __dadd_rn(__dmul_rn(jb.uh[0], uu), __dmul_rn(jb.vh[0], vv));
+                    y = __dadd_rn(__dmul_rn(jb.uh[1], uu), __dmul_rn(jb.vh[1], vv));
+                    z = __dadd_rn(__dmul_rn(jb.uh[2], uu), __dmul_rn(jb.vh[2], vv));
                 }
-                if (!(isfinite(prx[k]) && isfinite(pry[k]) && isfinite(prz[k]))) {
-                    bad = true;
-                    act[k] = false;
-                } else {
-                    mn[0] = fmin(mn[0], prx[k]); mx[0] = fmax(mx[0], prx[k]);
-                    mn[1] = fmin(mn[1], pry[k]); mx[1] = fmax(mx[1], pry[k]);
-                    mn[2] = fmin(mn[2], prz[k]); mx[2] = fmax(mx[2], prz[k]);
+                if (isfinite(x) && isfinite(y) && isfinite(z)) {
+                    // the same f32 offsets the tile set-up measured rho on
+                    dx[k] = kcf * (float)(x - ti.rc[0]);
+                    dy[k] = kcf * (float)(y - ti.rc[1]);
+                    dz[k] = kcf * (float)(z - ti.rc[2]);
+                    nd2[k] = -fmaf(dx[k], dx[k], fmaf(dy[k], dy[k], dz[k] * dz[k]));
                 }
             }
         }
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            const double a = warp_min(mn[d]), b = warp_max(mx[d]);
-            if (lane == 0) { sred[d][warp] = a; sred[3 + d][warp] = b; }
-        }
-        __syncthreads();
-        double rc[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            double a = DBL_MAX, b = -DBL_MAX;
-            for (int w = 0; w < kNT / 32; ++w) { a = fmin(a, sred[d][w]); b = fmax(b, sred[3 + d][w]); }
-            rc[d] = a <= b ? 0.5 * (a + b) : 0.0;
-        }
-        // ---- offsets, radius, final phase exp(+j k_c dr(pixel, P/2)) ----
-        float dx[PPT], dy[PPT], dz[PPT], nd2[PPT];
-        float rho = 0.0f;
-        const double4 pmid = jb.pulse[P / 2];
-        const double k_c = jb.sc->k_c;
-        const double kc2pi = k_c * kInv2Pi;
-#pragma unroll
-        for (int k = 0; k < PPT; ++k) {
-            dx[k] = dy[k] = dz[k] = nd2[k] = 0.0f;
-            float2 f = make_float2(0.f, 0.f);
-            if (act[k]) {
-                dx[k] = (float)(prx[k] - rc[0]);
-                dy[k] = (float)(pry[k] - rc[1]);
-                dz[k] = (float)(prz[k] - rc[2]);
-                const float d2 = fmaf(dx[k], dx[k], fmaf(dy[k], dy[k], dz[k] * dz[k]));
-                nd2[k] = -d2;
-                rho = fmaxf(rho, sqrtf(d2));
-                const double ex = prx[k] - pmid.x, ey = pry[k] - pmid.y, ez = prz[k] - pmid.z;
-                const double drm = pmid.w - sqrt(ex * ex + ey * ey + ez * ez);
-                double th = drm * kc2pi;
-                th = th - rint(th);
-                float s, c;
-                sincospif(2.0f * (float)th, &s, &c);
-                f = make_float2(c, s);
-            }
-            fin[tid + k * kNT] = f;
-        }
-        {
-            float m = rho;
-            for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-            if (lane == 0) sredf[warp] = m;
-        }
-        if (__syncthreads_or(bad) && tid == 0) atomicOr(&jb.sc->status, kStatusNonFinite);
-        float rho_t = 0.0f;
-        for (int w = 0; w < kNT / 32; ++w) rho_t = fmaxf(rho_t, sredf[w]);
-        rho_t = rho_t * (1.0f + 1e-5f) + 1e-6f;
-
-        const float inv_lsr = (float)jb.inv_lsr;
-        const float kc = (float)k_c;
-        const int K = (int)ceilf(rho_t * inv_lsr * 1.004f) + 2;
-        const int W = 2 * K + 1;
-        int C = stage_cap / W;
-        if (C > cmax) C = cmax;
-        if (C > P) C = P;
-        float ar[PPT], ai[PPT];
-#pragma unroll
-        for (int k = 0; k < PPT; ++k) ar[k] = ai[k] = 0.0f;
-
-        if (C < 1) {
+        if (sh.C < 1) {
             if (tid == 0) atomicOr(&jb.sc->status, kStatusTileTooWide);
         } else {
-            for (int p0 = 0; p0 < P; p0 += C) {
-                const int nc = min(C, P - p0);
-                // ---- per-pulse constants of this chunk (f64) ----
-                bool need3 = false, need_exact = false;
-                if (tid < nc) {
-                    const int p = p0 + tid;
-                    const double4 g = jb.pulse[p];
-                    const double wx = g.x - rc[0], wy = g.y - rc[1], wz = g.z - rc[2];
-                    const double R = sqrt(wx * wx + wy * wy + wz * wz);
-                    const double drc = g.w - R;
-                    double tc = (drc - jb.lsa) * jb.inv_lsr;
-                    tc = fmin(fmax(tc, -1.0e8), 1.0e8);
-                    const double fl = floor(tc);
-                    PulseA A;
-                    PulseB Bq;
-                    float2 Bp;
-                    int base;
-                    if (isfinite(R) && R > 0.0 && isfinite(tc)) {
-                        const double iR = 1.0 / R;
-                        A.wx = (float)(wx * iR); A.wy = (float)(wy * iR); A.wz = (float)(wz * iR);
-                        A.e = (float)(0.5 * iR);
-                        Bq.c0 = (float)((tc - fl) + ((double)K - 0.5));
-                        Bq.R = (float)R;
-                        base = (int)fl - K;
-                        double th = drc * kc2pi;
-                        th = th - rint(th);
-                        float s, c;
-                        sincospif(2.0f * (float)th, &s, &c);
-                        Bp = make_float2(c, -s);
-                        const float gm = rho_t * A.e;  // max |g|
-                        const float e2 = 2.0f * rho_t * gm * gm * kc;
-                        const float e3 = 5.0f * rho_t * gm * gm * gm * kc;
-                        need3 = e2 > kPhaseTol;
-                        need_exact = e3 > kPhaseTol || gm > 1e-3f;
-                    } else {
-                        A.wx = A.wy = A.wz = A.e = 0.0f;
-                        Bq.c0 = (float)K - 0.5f;
-                        Bq.R = 1.0f;
-                        base = 0;
-                        Bp = make_float2(0.f, 0.f);
-                        atomicOr(&jb.sc->status, kStatusNonFinite);
-                    }
-                    Bq.off = tid * W;
-                    Bq.pad = 0;
-                    pa[tid] = A;
-                    pb[tid] = Bq;
-                    pB[tid] = Bp;
-                    pbase[tid] = base;
-                }
-                const int mode = __syncthreads_or(need_exact) ? 2 : (__syncthreads_or(need3) ? 1 : 0);
-                // ---- stage the chunk's range windows: (m, d) * B ----
-                for (int i = warp; i < nc; i += kNT / 32) {
-                    const float2 *__restrict__ q = jb.Q + (size_t)(p0 + i) * N;
-                    const int base = pbase[i];
-                    const float2 B = pB[i];
-                    float4 *dst = stage + i * W;
-                    for (int j = lane; j < W; j += 32) {
-                        const int g0 = min(max(base + j, 0), N - 1);
-                        const int g1 = min(max(base + j + 1, 0), N - 1);
-                        const float2 a = __ldg(&q[g0]);
-                        const float2 b = __ldg(&q[g1]);
-                        const float mr = 0.5f * (a.x + b.x), mi = 0.5f * (a.y + b.y);
-                        const float dr = b.x - a.x, di = b.y - a.y;
-                        dst[j] = make_float4(fmaf(mr, B.x, -mi * B.y), fmaf(mr, B.y, mi * B.x),
-                                             fmaf(dr, B.x, -di * B.y), fmaf(dr, B.y, di * B.x));
-                    }
-                }
-                __syncthreads();
-                const float hi = (float)(W - 1) - 0.5f;
-                if (mode == 0)
-                    accumulate<0, PPT>(nc, pa, pb, stage, inv_lsr, kc, hi, dx, dy, dz, nd2, ar, ai);
-                else if (mode == 1)
-                    accumulate<1, PPT>(nc, pa, pb, stage, inv_lsr, kc, hi, dx, dy, dz, nd2, ar, ai);
-                else
-                    accumulate<2, PPT>(nc, pa, pb, stage, inv_lsr, kc, hi, dx, dy, dz, nd2, ar, ai);
-                __syncthreads();
+            const float ilk = (float)(jb.inv_lsr / k_c);  // range bins per radian of Delta
+            const float hi = (float)(sh.W - 1) - 0.5f;
+            const uint32_t pstride = (uint32_t)sh.W * 16u;
+            for (int c = 0; c < sh.nchunks; ++c) {
+                const int b = c & 1;
+                bar_sync(kBarFull0 + b);
+                const int p0 = c * sh.C;
+                accumulate_any<PPT>(sm.s_mode[b], ti.planar != 0, min(sh.C, P - p0), sm.rec + b * cmax,
+                                    stage_base + (uint32_t)(b * stage_cap) * 16u, pstride, ilk, hi, dx, dy,
+                                    dz, nd2, ar, ai);
+                bar_arrive(kBarEmpty0 + b);
             }
         }
-        // ---- epilogue: final phase, row flip (backprojection.cpp:130-138), max|z| ----
+        // ---- final phase, row flip (backprojection.cpp:130-138), max|z| ----
         double zmax = 0.0;
 #pragma unroll
         for (int k = 0; k < PPT; ++k) {
             const int ix = tx0 + lx, iy = ty0 + ly + k * ROWS;
             if (ix < nu && iy < nv) {
-                const float2 f = fin[tid + k * kNT];
+                const float2 f = jb.fin[(long long)iy * nu + ix];
                 const double zr = (double)fmaf(ar[k], f.x, -ai[k] * f.y);
                 const double zi = (double)fmaf(ar[k], f.y, ai[k] * f.x);
                 jb.out[(long long)(nv - 1 - iy) * nu + ix] = make_double2(zr, zi);
@@ -339,16 +367,48 @@ __global__ void __launch_bounds__(kNT) bp_tile_kernel(const DevJob *__restrict__
             }
         }
         zmax = warp_max(zmax);
-        if (lane == 0) sred[0][warp] = zmax;
+        if (lane == 0) sm.sred[warp] = zmax;
         __syncthreads();
         if (tid == 0) {
             double m = 0.0;
-            for (int w = 0; w < kNT / 32; ++w) m = fmax(m, sred[0][w]);
+            for (int w = 0; w < kConsumerWarps; ++w) m = fmax(m, sm.sred[w]);
             atomicMax(&jb.sc->maxabs, (unsigned long long)__double_as_longlong(m));
         }
-        __syncthreads();
         if (!persistent) break;
     }
+}
+
+// MINB: CTAs per SM the register allocation targets (2 or 3).  The role
+// test reads the thread index through a shuffle from lane 0 so the compiler
+// sees a warp-uniform branch and allocates the two roles' registers apart.
+template <int TX, int TY, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) bp_tile_kernel(const DevJob *__restrict__ jobs,
+                                                                 const WorkItem *__restrict__ items,
+                                                                 int nitems, int *__restrict__ counter,
+                                                                 int stage_cap, int cmax, int persistent) {
+    static_assert(TX * TY % kConsumers == 0, "tile must be a multiple of the consumers");
+    extern __shared__ float4 smem[];
+    __shared__ double sred[kConsumerWarps];
+    __shared__ int s_item, s_mode[2];
+    __shared__ uint64_t mbar[4];
+    TileSmem sm;
+    sm.stage = smem;
+    sm.rec = reinterpret_cast<PulseRec *>(smem + 2 * stage_cap);
+    sm.mbar_rec = mbar;
+    sm.mbar_win = mbar + 2;
+    sm.sred = sred;
+    sm.s_item = &s_item;
+    sm.s_mode = s_mode;
+    if (threadIdx.x == kConsumers) {
+        for (int i = 0; i < 4; ++i)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[i])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (__shfl_sync(0xffffffffu, (int)threadIdx.x, 0) >= kConsumers)
+        producer_loop(jobs, items, nitems, stage_cap, cmax, persistent, sm);
+    else
+        consumer_loop<TX, TY>(jobs, items, nitems, counter, stage_cap, cmax, persistent, sm);
 }
 
 // ---- naive FP32 kernel: one thread per pixel ----
@@ -377,10 +437,9 @@ __global__ void __launch_bounds__(256) bp_naive_kernel(const DevJob *__restrict_
         const float fl = floorf(t);
         const int l = (int)fminf(fmaxf(fl, -2.0f), (float)N + 1.0f);
         const float w = fminf(fmaxf(t - fl, 0.f), 1.f);
-        const int l0 = min(max(l, 0), N - 1), l1 = min(max(l + 1, 0), N - 1);
-        const float2 *q = jb.Q + (size_t)p * N;
-        const float2 a = __ldg(&q[l0]), b = __ldg(&q[l1]);
-        const float vr = fmaf(w, b.x - a.x, a.x), vi = fmaf(w, b.y - a.y, a.y);
+        // pair l holds (m, d) of bins (l, l+1); below the profile it is (Q[0], 0)
+        const float4 md = __ldg(&jb.Qp[(size_t)p * (N + 1) + (l < 0 ? N : min(l, N - 1))]);
+        const float vr = fmaf(w - 0.5f, md.z, md.x), vi = fmaf(w - 0.5f, md.w, md.y);
         float s, c;
         __sincosf(kc * dr, &s, &c);
         ar = fmaf(vr, c, fmaf(vi, s, ar));
@@ -393,44 +452,50 @@ __global__ void __launch_bounds__(256) bp_naive_kernel(const DevJob *__restrict_
     __sincosf(kc * drm, &s, &c);
     const double zr = (double)(ar * c - ai * s), zi = (double)(ar * s + ai * c);
     jb.out[(long long)(jb.nv - 1 - iy) * jb.nu + ix] = make_double2(zr, zi);
-    atomicMax(&jb.sc->maxabs, (unsigned long long)__double_as_longlong(sqrt(zr * zr + zi * zi)));
+    double m = sqrt(zr * zr + zi * zi);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(__activemask(), m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&jb.sc->maxabs, (unsigned long long)__double_as_longlong(m));
 }
 
-template <int TX, int TY>
+template <int TX, int TY, int MINB>
 cudaError_t set_attr(size_t smem) {
-    return cudaFuncSetAttribute(bp_tile_kernel<TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(bp_tile_kernel<TX, TY, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem);
 }
 
-template <int TX, int TY>
+template <int TX, int TY, int MINB>
 int active_blocks(size_t smem) {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bp_tile_kernel<TX, TY>, kNT, smem) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bp_tile_kernel<TX, TY, MINB>, kThreads, smem) !=
+        cudaSuccess)
         return 0;
     return n;
 }
 
 }  // namespace
 
-bool bp_tile_supported(int tx, int ty) {
-    return (tx == 32 && (ty == 8 || ty == 16 || ty == 32 || ty == 64)) ||
-           (tx == 64 && (ty == 16 || ty == 32)) || (tx == 16 && (ty == 16 || ty == 32 || ty == 64));
+// (tile width, tile height, CTAs per SM) instantiations of bp_tile_kernel
+#define SARBP_BP_TILES(X)                                                                      \
+    X(32, 8, 2) X(32, 16, 2) X(32, 32, 2) X(32, 64, 2) X(64, 16, 2) X(64, 32, 2) X(16, 16, 2)      \
+    X(16, 32, 2) X(16, 64, 2) X(32, 8, 3) X(32, 16, 3) X(32, 32, 3) X(64, 16, 3) X(16, 32, 3)
+
+bool bp_tile_supported(int tx, int ty, int minb) {
+#define X(a, b, m) \
+    if (tx == a && ty == b && minb == m) return true;
+    SARBP_BP_TILES(X)
+#undef X
+    return false;
 }
 
 size_t bp_smem_bytes(const BpLaunch &L) {
-    return (size_t)L.stage_cap * sizeof(float4) +
-           (size_t)L.cmax * (sizeof(PulseA) + sizeof(PulseB) + sizeof(float2) + sizeof(int)) +
-           (size_t)L.tile_x * L.tile_y * sizeof(float2);
+    return 2 * (size_t)L.stage_cap * sizeof(float4) + 2 * (size_t)L.cmax * sizeof(PulseRec);
 }
 
-#define SARBP_BP_TILES(X)                                                                      \
-    X(32, 8) X(32, 16) X(32, 32) X(32, 64) X(64, 16) X(64, 32) X(16, 16) X(16, 32) X(16, 64)
-
 cudaError_t init_backproject_attributes() {
-    const size_t maxs = 200 * 1024;
+    const size_t maxs = 220 * 1024;
     cudaError_t e = cudaSuccess;
-#define X(a, b) \
-    if (e == cudaSuccess) e = set_attr<a, b>(maxs);
+#define X(a, b, m) \
+    if (e == cudaSuccess) e = set_attr<a, b, m>(maxs);
     SARBP_BP_TILES(X)
 #undef X
     return e;
@@ -438,8 +503,8 @@ cudaError_t init_backproject_attributes() {
 
 int bp_max_active_blocks(const BpLaunch &L) {
     const size_t smem = bp_smem_bytes(L);
-#define X(a, b) \
-    if (L.tile_x == a && L.tile_y == b) return active_blocks<a, b>(smem);
+#define X(a, b, m) \
+    if (L.tile_x == a && L.tile_y == b && L.minb == m) return active_blocks<a, b, m>(smem);
     SARBP_BP_TILES(X)
 #undef X
     return 0;
@@ -450,11 +515,11 @@ cudaError_t launch_backproject(const BpLaunch &L, const DevJob *d_jobs, const Wo
     const size_t smem = bp_smem_bytes(L);
     const int grid = L.persistent ? L.grid : nitems;
     if (grid <= 0) return cudaSuccess;
-#define X(a, b)                                                                              \
-    if (L.tile_x == a && L.tile_y == b) {                                                    \
-        bp_tile_kernel<a, b><<<grid, kNT, smem, st>>>(d_jobs, d_items, nitems, d_counter,    \
-                                                      L.stage_cap, L.cmax, L.persistent);    \
-        return cudaGetLastError();                                                           \
+#define X(a, b, m)                                                                                \
+    if (L.tile_x == a && L.tile_y == b && L.minb == m) {                                          \
+        bp_tile_kernel<a, b, m><<<grid, kThreads, smem, st>>>(d_jobs, d_items, nitems, d_counter, \
+                                                              L.stage_cap, L.cmax, L.persistent); \
+        return cudaGetLastError();                                                                \
     }
     SARBP_BP_TILES(X)
 #undef X

@@ -1,0 +1,189 @@
+// geometry.cu -- f64 geometry of the pixel tiles, ahead of the FP32 loop.
+//
+// tile_setup_kernel (one CTA per (job, tile)):
+//   rc    = centre of the bounding box of the tile's pixel positions
+//   rho   = max |(f32)(r - rc)|, the same f32 offsets the backprojection
+//           kernel forms, padded; K = ceil(1.004 rho / lsr) + 2
+//   fin   = exp(+j k_c dr(pixel, P/2)) per pixel (backprojection.cpp:135),
+//           dr = |pos| - |r - pos| in f64, phase reduced in f64
+// pulse_record_kernel (one thread per (tile, pulse)):
+//   w = pos - rc, R = |w|, dr_c = |pos| - R, t_c = (dr_c - lsa) / lsr,
+//   base = floor(t_c) - K, theta = k_c dr_c reduced to [-pi, pi),
+//   c0 = t_c - floor(t_c) + K - 1/2 - theta / (k_c lsr), and the series
+//   order the pulse needs for the tile radius (see backproject.cu).
+#include <cfloat>
+
+#include "internal.h"
+#include "kernels.h"
+
+namespace sarbp {
+
+namespace {
+
+constexpr int kThreadsGeom = 256;
+constexpr double kInv2Pi = 0.15915494309189533577;
+constexpr double kTwoPi = 6.28318530717958647693;
+constexpr float kPhaseTol = 2e-5f;  // rad, truncation budget of the series
+
+__device__ __forceinline__ void pixel_pos(const DevJob &jb, int ix, int iy, double &x, double &y,
+                                          double &z) {
+    if (jb.r) {
+        const long long npix = (long long)jb.nu * jb.nv;
+        const long long pix = (long long)iy * jb.nu + ix;
+        x = jb.r[pix];
+        y = jb.r[npix + pix];
+        z = jb.r[2 * npix + pix];
+    } else {
+        // img_plane.cpp:92-102: (0 + u_hat*u) + v_hat*v
+        const double uu = jb.u[ix], vv = jb.v[iy];
+        x = __dadd_rn(__dmul_rn(jb.uh[0], uu), __dmul_rn(jb.vh[0], vv));
+        y = __dadd_rn(__dmul_rn(jb.uh[1], uu), __dmul_rn(jb.vh[1], vv));
+        z = __dadd_rn(__dmul_rn(jb.uh[2], uu), __dmul_rn(jb.vh[2], vv));
+    }
+}
+
+template <class T, class Op>
+__device__ T block_reduce(T v, T *sbuf, Op op) {
+    for (int o = 16; o > 0; o >>= 1) v = op(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0) sbuf[warp] = v;
+    __syncthreads();
+    v = sbuf[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) v = op(v, sbuf[w]);
+    return v;
+}
+
+struct MinOp { __device__ double operator()(double a, double b) const { return fmin(a, b); } };
+struct MaxOp { __device__ double operator()(double a, double b) const { return fmax(a, b); } };
+struct MaxOpF { __device__ float operator()(float a, float b) const { return fmaxf(a, b); } };
+struct AndOp { __device__ int operator()(int a, int b) const { return a & b; } };
+struct OrOp { __device__ int operator()(int a, int b) const { return a | b; } };
+
+__global__ void __launch_bounds__(kThreadsGeom) tile_setup_kernel(const DevJob *__restrict__ jobs,
+                                                                  const WorkItem *__restrict__ items) {
+    __shared__ double sd[32];
+    __shared__ float sf[32];
+    __shared__ int si[32];
+    const WorkItem wi = items[blockIdx.x];
+    const DevJob &jb = jobs[wi.job];
+    const int TX = jb.tile_x, TY = jb.tile_y;
+    const int tx0 = (wi.tile % jb.tiles_x) * TX, ty0 = (wi.tile / jb.tiles_x) * TY;
+    double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    int bad = 0;
+    for (int idx = threadIdx.x; idx < TX * TY; idx += blockDim.x) {
+        const int ix = tx0 + idx % TX, iy = ty0 + idx / TX;
+        if (ix >= jb.nu || iy >= jb.nv) continue;
+        double x, y, z;
+        pixel_pos(jb, ix, iy, x, y, z);
+        if (!(isfinite(x) && isfinite(y) && isfinite(z))) {
+            bad = 1;
+            continue;
+        }
+        mn[0] = fmin(mn[0], x); mx[0] = fmax(mx[0], x);
+        mn[1] = fmin(mn[1], y); mx[1] = fmax(mx[1], y);
+        mn[2] = fmin(mn[2], z); mx[2] = fmax(mx[2], z);
+    }
+    double rc[3];
+    for (int d = 0; d < 3; ++d) {
+        const double a = block_reduce(mn[d], sd, MinOp()), b = block_reduce(mx[d], sd, MaxOp());
+        rc[d] = a <= b ? 0.5 * (a + b) : 0.0;
+    }
+    const double k_c = jb.sc->k_c;
+    const double4 pm = jb.pulse[jb.P / 2];
+    float rho = 0.0f;
+    int planar = 1;
+    for (int idx = threadIdx.x; idx < TX * TY; idx += blockDim.x) {
+        const int ix = tx0 + idx % TX, iy = ty0 + idx / TX;
+        if (ix >= jb.nu || iy >= jb.nv) continue;
+        double x, y, z;
+        pixel_pos(jb, ix, iy, x, y, z);
+        float2 f = make_float2(0.f, 0.f);
+        if (isfinite(x) && isfinite(y) && isfinite(z)) {
+            const float ox = (float)(x - rc[0]), oy = (float)(y - rc[1]), oz = (float)(z - rc[2]);
+            rho = fmaxf(rho, sqrtf(fmaf(ox, ox, fmaf(oy, oy, oz * oz))));
+            planar &= (oz == 0.0f);
+            const double ex = x - pm.x, ey = y - pm.y, ez = z - pm.z;
+            const double drm = pm.w - sqrt(ex * ex + ey * ey + ez * ez);
+            double th = drm * (k_c * kInv2Pi);
+            th = th - rint(th);
+            float s, c;
+            sincospif(2.0f * (float)th, &s, &c);
+            f = make_float2(c, s);
+        }
+        jb.fin[(long long)iy * jb.nu + ix] = f;
+    }
+    rho = block_reduce(rho, sf, MaxOpF());
+    planar = block_reduce(planar, si, AndOp());
+    bad = block_reduce(bad, si, OrOp());
+    if (threadIdx.x == 0) {
+        TileInfo t;
+        t.rc[0] = rc[0];
+        t.rc[1] = rc[1];
+        t.rc[2] = rc[2];
+        t.rho = rho * (1.0f + 1e-5f) + 1e-6f;
+        t.K = (int)ceilf(t.rho * (float)jb.inv_lsr * 1.004f) + 2;
+        t.planar = planar;
+        t.pad = 0;
+        jb.tiles[wi.tile] = t;
+        if (bad) atomicOr(&jb.sc->status, kStatusNonFinite);
+    }
+}
+
+// blockIdx.x = work item, blockIdx.y * blockDim.x + threadIdx.x = pulse
+__global__ void __launch_bounds__(kThreadsGeom) pulse_record_kernel(const DevJob *__restrict__ jobs,
+                                                                    const WorkItem *__restrict__ items) {
+    const WorkItem wi = items[blockIdx.x];
+    const DevJob &jb = jobs[wi.job];
+    const int p = blockIdx.y * blockDim.x + threadIdx.x;
+    if (p >= jb.P) return;
+    const TileInfo t = jb.tiles[wi.tile];
+    const double k_c = jb.sc->k_c;
+    const double4 g = jb.pulse[p];
+    const double wx = g.x - t.rc[0], wy = g.y - t.rc[1], wz = g.z - t.rc[2];
+    const double R = sqrt(wx * wx + wy * wy + wz * wz);
+    const double drc = g.w - R;
+    double tc = (drc - jb.lsa) * jb.inv_lsr;
+    tc = fmin(fmax(tc, -1.0e8), 1.0e8);
+    const double fl = floor(tc);
+    PulseRec rec;
+    if (isfinite(R) && R > 0.0 && isfinite(tc)) {
+        const double iR = 1.0 / R;
+        double th = drc * (k_c * kInv2Pi);
+        th = th - rint(th);
+        const double theta = kTwoPi * th;  // in [-pi, pi]
+        const float gm = (float)(t.rho * 0.5 * iR);                    // max |g| = rho / (2R)
+        const float kcf = (float)k_c;
+        const float e2 = 2.0f * t.rho * gm * gm * kcf;                 // 2-term truncation (rad)
+        const float e3 = 5.0f * t.rho * gm * gm * gm * kcf;            // 3-term truncation (rad)
+        const int order = (e3 > kPhaseTol || gm > 1e-3f) ? 2 : (e2 > kPhaseTol ? 1 : 0);
+        const int base = (int)fl - t.K;
+        rec.a = make_float4((float)(wx * iR), (float)(wy * iR), (float)(wz * iR), (float)(0.5 * iR / k_c));
+        const double c0 = (tc - fl) + ((double)t.K - 0.5) - theta * (jb.inv_lsr / k_c);
+        rec.b = make_float4((float)c0, (float)theta, (float)(k_c * R), __int_as_float(4 * base + order));
+    } else {
+        // no contribution: the staging leaves this pulse's window at zero
+        rec.a = make_float4(0.f, 0.f, 0.f, 0.f);
+        rec.b = make_float4((float)t.K - 0.5f, 0.f, 1.f, __int_as_float(3));
+        atomicOr(&jb.sc->status, kStatusNonFinite);
+    }
+    jb.recs[(size_t)wi.tile * jb.P + p] = rec;
+}
+
+}  // namespace
+
+cudaError_t launch_tile_setup(const DevJob *d_jobs, const WorkItem *d_items, int nitems, cudaStream_t st) {
+    if (nitems <= 0) return cudaSuccess;
+    tile_setup_kernel<<<nitems, kThreadsGeom, 0, st>>>(d_jobs, d_items);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pulse_records(const DevJob *d_jobs, const WorkItem *d_items, int nitems, int max_p,
+                                 cudaStream_t st) {
+    if (nitems <= 0) return cudaSuccess;
+    const dim3 grid(nitems, (max_p + kThreadsGeom - 1) / kThreadsGeom);
+    pulse_record_kernel<<<grid, kThreadsGeom, 0, st>>>(d_jobs, d_items);
+    return cudaGetLastError();
+}
+
+}  // namespace sarbp

@@ -2,8 +2,9 @@
 //
 // One DevJob describes one image-formation job in device memory: the
 // caller's inputs, the library's per-job scratch (range profiles, windows,
-// per-pulse geometry) and the outputs.  The host builds an array of them,
-// copies it to the device, and every kernel of a batch indexes it by job.
+// per-pulse and per-tile geometry) and the outputs.  The host builds an
+// array of them, copies it to the device, and every kernel of a batch
+// indexes it by job.
 #pragma once
 
 #include <cstdint>
@@ -15,10 +16,11 @@ constexpr int kMaxTaylorTerms = 64;  // n_bar - 1 <= 64  (S_L up to ~150 dB)
 constexpr int kMinLogN = 4;          // N_fft in [16, 16384]
 constexpr int kMaxLogN = 14;
 
-// status bits written by kernels into DevJob::status
+// status bits written by kernels into JobScalars::status
 constexpr int kStatusTileTooWide = 1;   // range window of a tile exceeds smem
 constexpr int kStatusNonFinite = 2;     // non-finite pixel or pulse geometry
 constexpr int kStatusNearField = 4;     // pulse closer than the tile radius
+constexpr int kStatusTimeout = 8;       // a bounded wait on an async copy gave up
 
 // per-job words the kernels write; kept contiguous for one status read-back
 struct JobScalars {
@@ -26,6 +28,23 @@ struct JobScalars {
     double k_c;                 // k_r[S/2] by precision mode (prep kernel)
     int status;                 // kStatus* bits
     int pad[3];
+};
+
+// Geometry of one pixel tile (tile-set-up kernel -> backprojection).
+struct __align__(16) TileInfo {
+    double rc[3];  // centre of the tile's bounding box
+    float rho;     // max |r - rc| over the tile, padded (m)
+    int K;         // range window half-width (bins): W = 2K + 1
+    int planar;    // 1 when every pixel has r.z == rc.z
+    int pad;
+};
+
+// Per-(tile, pulse) constants (pulse-record kernel -> backprojection):
+//   a = (w_hat.x, w_hat.y, w_hat.z, e = 1/(2 k_c R))
+//   b = (c0 - theta*inv_lsr/k_c, theta, k_c R, int bits: 4*base + series order)
+struct __align__(16) PulseRec {
+    float4 a;
+    float4 b;
 };
 
 struct DevJob {
@@ -46,11 +65,15 @@ struct DevJob {
     const double *u, *v;  // grid form
     double uh[3], vh[3];
     // library scratch (device)
-    float2 *Q;            // [P][N] range profiles
+    float2 *Q;            // [P][N] range profiles (only when Qp is null)
+    float4 *Qp;           // [P][N+1] interpolation pairs (m, d) + (Q[0], 0) at N
     float *filt;          // [S]  |k_r|
     float *wS;            // [S]  sample window
     float *wP;            // [P]  pulse window
     double4 *pulse;       // [P]  (x, y, z, |pos|) by precision mode
+    TileInfo *tiles;      // [tiles_x * tiles_y]
+    PulseRec *recs;       // [tiles][P]
+    float2 *fin;          // [nv][nu] exp(+j k_c dr(pixel, P/2)), r-space order
     JobScalars *sc;       // max|z|, k_c, status (written by the kernels)
     // constants
     double delta_r, lsa, lsr, inv_lsr;
@@ -61,7 +84,7 @@ struct DevJob {
     double dB_min, dB_max;
 };
 
-// (job, tile) work item of the persistent backprojection launch
+// (job, tile) work item of the per-tile kernels
 struct WorkItem {
     int job;
     int tile;

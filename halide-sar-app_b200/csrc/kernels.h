@@ -18,25 +18,31 @@ void launch_prep(const DevJob *d_jobs, int njobs, cudaStream_t st);
 // range_compress.cu
 int twiddle_table_size(int logN);
 void fill_twiddle_table(int logN, float2 *host);
-cudaError_t launch_range_compress(int logN, const DevJob *d_jobs, const RowItem *d_rows, int nrows,
+cudaError_t launch_range_compress(int logN, const DevJob *d_jobs, const RowItem *d_rows, int nrows, int pairs,
                                   const float2 *d_tw, cudaStream_t st);
 cudaError_t init_range_compress_attributes();
 
 // backproject.cu
 struct BpLaunch {
     int tile_x, tile_y;
-    int stage_cap;   // float4 entries of the staging buffer
+    int minb;        // CTAs per SM the kernel's registers are sized for (2 or 3)
+    int stage_cap;   // float4 entries of each half of the staging double buffer
     int cmax;        // max pulses per chunk
     int persistent;  // 1: grid = resident CTAs pulling items from *counter
     int grid;        // CTAs when persistent
 };
-bool bp_tile_supported(int tile_x, int tile_y);
+bool bp_tile_supported(int tile_x, int tile_y, int minb);
 size_t bp_smem_bytes(const BpLaunch &L);
 int bp_max_active_blocks(const BpLaunch &L);
 cudaError_t init_backproject_attributes();
 cudaError_t launch_backproject(const BpLaunch &L, const DevJob *d_jobs, const WorkItem *d_items,
                                int nitems, int *d_counter, cudaStream_t st);
 cudaError_t launch_backproject_naive(const DevJob *d_jobs, int job, int nu, int nv, cudaStream_t st);
+
+// geometry.cu
+cudaError_t launch_tile_setup(const DevJob *d_jobs, const WorkItem *d_items, int nitems, cudaStream_t st);
+cudaError_t launch_pulse_records(const DevJob *d_jobs, const WorkItem *d_items, int nitems, int max_p,
+                                 cudaStream_t st);
 
 // peaks.cu
 cudaError_t measure_peaks(int num_sms, cudaStream_t st, double *ffma_per_s, double *mufu_per_s);

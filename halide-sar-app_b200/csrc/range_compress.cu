@@ -144,17 +144,40 @@ struct Plan {
     static constexpr int NP16 = L / 4;
 };
 
-// Recursive radix-16 passes; pass index K has NS = R0 * 16^K.
+// Recursive radix-16 passes; pass index K has NS = R0 * 16^K.  The last
+// pass stores with the fftshift, either the profile itself (qrow) or, with
+// `pairs`, the interpolation pairs (m, d) = ((Q[k] + Q[k+1]) / 2,
+// Q[k+1] - Q[k]) with Q[N] read as Q[N-1] (the reference's index clamp),
+// followed by (Q[0], 0) at index N.
 template <int N, int NS>
 __device__ __forceinline__ void passes16(float2 (&v)[16], int t, float2 *sm, const float2 *tw_base,
-                                         int tw_off, float2 *__restrict__ qrow) {
+                                         int tw_off, float2 *__restrict__ qrow, float4 *__restrict__ prow,
+                                         bool pairs) {
     constexpr int R = 16;
     const float2 *tw = tw_base + tw_off;
     pass_compute<N, R, NS>(v, t, tw);
     if constexpr (NS * R == N) {
         // last pass: j < NS, out index k = j + r*NS, stored with fftshift
         const int j = t;
-        if (qrow != nullptr) {
+        if (pairs) {
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < R; ++r) sm[pad_idx((j + r * NS + N / 2) & (N - 1))] = v[r];
+            __syncthreads();
+            if (prow != nullptr) {
+#pragma unroll
+                for (int u = 0; u < R; ++u) {
+                    const int k = t + u * NS;
+                    const float2 a = sm[pad_idx(k)];
+                    const float2 b = sm[pad_idx(k + 1 < N ? k + 1 : N - 1)];
+                    prow[k] = make_float4(0.5f * (a.x + b.x), 0.5f * (a.y + b.y), b.x - a.x, b.y - a.y);
+                }
+                if (t == 0) {
+                    const float2 a = sm[pad_idx(0)];
+                    prow[N] = make_float4(a.x, a.y, 0.f, 0.f);
+                }
+            }
+        } else if (qrow != nullptr) {
 #pragma unroll
             for (int r = 0; r < R; ++r) qrow[(j + r * NS + N / 2) & (N - 1)] = v[r];
         }
@@ -163,14 +186,14 @@ __device__ __forceinline__ void passes16(float2 (&v)[16], int t, float2 *sm, con
         pass_store_smem<N, R, NS>(v, t, sm);
         __syncthreads();
         pass_load_smem<N, R>(v, t, sm);
-        passes16<N, NS * R>(v, t, sm, tw_base, tw_off + (NS > 1 ? (R - 1) * NS : 0), qrow);
+        passes16<N, NS * R>(v, t, sm, tw_base, tw_off + (NS > 1 ? (R - 1) * NS : 0), qrow, prow, pairs);
     }
 }
 
 template <int LOGN>
 __global__ void __launch_bounds__((1 << LOGN) / 16 > 256 ? (1 << LOGN) / 16 : 256)
 range_compress_kernel(const DevJob *__restrict__ jobs, const RowItem *__restrict__ rows, int nrows,
-                      const float2 *__restrict__ tw) {
+                      const float2 *__restrict__ tw, int pairs) {
     constexpr int N = 1 << LOGN;
     constexpr int T = N / 16;
     constexpr int RPB = T >= 256 ? 1 : 256 / T;
@@ -212,18 +235,18 @@ range_compress_kernel(const DevJob *__restrict__ jobs, const RowItem *__restrict
             v[b * R1 + r] = x;
         }
     }
-    float2 *__restrict__ qrow = jb.Q + (size_t)p * N;
-    if (!live) qrow = nullptr;
+    float2 *__restrict__ qrow = (live && !pairs) ? jb.Q + (size_t)p * N : nullptr;
+    float4 *__restrict__ prow = (live && pairs) ? jb.Qp + (size_t)p * (N + 1) : nullptr;
     if constexpr (R0 > 1) {
         pass_compute<N, R0, 1>(v, t, tw);
         __syncthreads();
         pass_store_smem<N, R0, 1>(v, t, sm);
         __syncthreads();
         pass_load_smem<N, 16>(v, t, sm);
-        passes16<N, R0>(v, t, sm, tw, 0, qrow);
+        passes16<N, R0>(v, t, sm, tw, 0, qrow, prow, pairs != 0);
     } else {
         // first radix-16 pass has NS = 1 and no twiddles
-        passes16<N, 1>(v, t, sm, tw, 0, qrow);
+        passes16<N, 1>(v, t, sm, tw, 0, qrow, prow, pairs != 0);
     }
 }
 
@@ -263,7 +286,7 @@ void fill_twiddle_table(int logN, float2 *host) {
 }
 
 template <int LOGN>
-static cudaError_t launch_rc(const DevJob *d_jobs, const RowItem *d_rows, int nrows,
+static cudaError_t launch_rc(const DevJob *d_jobs, const RowItem *d_rows, int nrows, int pairs,
                              const float2 *d_tw, cudaStream_t st) {
     constexpr int N = 1 << LOGN;
     constexpr int T = N / 16;
@@ -271,7 +294,7 @@ static cudaError_t launch_rc(const DevJob *d_jobs, const RowItem *d_rows, int nr
     const int threads = RPB * T;
     const size_t smem = (size_t)RPB * (N + N / 16) * sizeof(float2);
     const int blocks = (nrows + RPB - 1) / RPB;
-    range_compress_kernel<LOGN><<<blocks, threads, smem, st>>>(d_jobs, d_rows, nrows, d_tw);
+    range_compress_kernel<LOGN><<<blocks, threads, smem, st>>>(d_jobs, d_rows, nrows, d_tw, pairs);
     return cudaGetLastError();
 }
 
@@ -301,20 +324,20 @@ cudaError_t init_range_compress_attributes() {
     return e;
 }
 
-cudaError_t launch_range_compress(int logN, const DevJob *d_jobs, const RowItem *d_rows, int nrows,
+cudaError_t launch_range_compress(int logN, const DevJob *d_jobs, const RowItem *d_rows, int nrows, int pairs,
                                   const float2 *d_tw, cudaStream_t st) {
     switch (logN) {
-        case 4: return launch_rc<4>(d_jobs, d_rows, nrows, d_tw, st);
-        case 5: return launch_rc<5>(d_jobs, d_rows, nrows, d_tw, st);
-        case 6: return launch_rc<6>(d_jobs, d_rows, nrows, d_tw, st);
-        case 7: return launch_rc<7>(d_jobs, d_rows, nrows, d_tw, st);
-        case 8: return launch_rc<8>(d_jobs, d_rows, nrows, d_tw, st);
-        case 9: return launch_rc<9>(d_jobs, d_rows, nrows, d_tw, st);
-        case 10: return launch_rc<10>(d_jobs, d_rows, nrows, d_tw, st);
-        case 11: return launch_rc<11>(d_jobs, d_rows, nrows, d_tw, st);
-        case 12: return launch_rc<12>(d_jobs, d_rows, nrows, d_tw, st);
-        case 13: return launch_rc<13>(d_jobs, d_rows, nrows, d_tw, st);
-        case 14: return launch_rc<14>(d_jobs, d_rows, nrows, d_tw, st);
+        case 4: return launch_rc<4>(d_jobs, d_rows, nrows, pairs, d_tw, st);
+        case 5: return launch_rc<5>(d_jobs, d_rows, nrows, pairs, d_tw, st);
+        case 6: return launch_rc<6>(d_jobs, d_rows, nrows, pairs, d_tw, st);
+        case 7: return launch_rc<7>(d_jobs, d_rows, nrows, pairs, d_tw, st);
+        case 8: return launch_rc<8>(d_jobs, d_rows, nrows, pairs, d_tw, st);
+        case 9: return launch_rc<9>(d_jobs, d_rows, nrows, pairs, d_tw, st);
+        case 10: return launch_rc<10>(d_jobs, d_rows, nrows, pairs, d_tw, st);
+        case 11: return launch_rc<11>(d_jobs, d_rows, nrows, pairs, d_tw, st);
+        case 12: return launch_rc<12>(d_jobs, d_rows, nrows, pairs, d_tw, st);
+        case 13: return launch_rc<13>(d_jobs, d_rows, nrows, pairs, d_tw, st);
+        case 14: return launch_rc<14>(d_jobs, d_rows, nrows, pairs, d_tw, st);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -22,17 +22,28 @@ int ilog2i(long long n) {
 }
 
 struct JobLayout {
-    size_t Q, filt, wS, wP, pulse, end;
+    size_t Q, Qp, filt, wS, wP, pulse, tiles, recs, fin, end;
 };
 
-JobLayout layout_of(const sarbp_job &j, size_t base) {
+// Scratch of one job: profiles (pairs for the tile kernel, plain Q for the
+// range-compression-only entry point), windows, pulse table, and for the
+// tile kernel the tile table, per-(tile, pulse) records and final phases.
+JobLayout layout_of(const sarbp_job &j, size_t base, int tile_x, int tile_y, bool rc_only, bool naive) {
     JobLayout L;
+    const size_t P = (size_t)j.npulses, N = (size_t)j.n_fft, S = (size_t)j.nsamples;
+    const bool tiles = !rc_only && !naive;
+    const size_t ntiles =
+        tiles ? (size_t)((j.nu + tile_x - 1) / tile_x) * (size_t)((j.nv + tile_y - 1) / tile_y) : 0;
     size_t o = base;
-    L.Q = o;      o = align_up(o + (size_t)j.npulses * j.n_fft * sizeof(float2), 256);
-    L.filt = o;   o = align_up(o + (size_t)j.nsamples * sizeof(float), 256);
-    L.wS = o;     o = align_up(o + (size_t)j.nsamples * sizeof(float), 256);
-    L.wP = o;     o = align_up(o + (size_t)j.npulses * sizeof(float), 256);
-    L.pulse = o;  o = align_up(o + (size_t)j.npulses * sizeof(double4), 256);
+    L.Q = o;      o = align_up(o + (rc_only ? P * N * sizeof(float2) : 0), 256);
+    L.Qp = o;     o = align_up(o + (rc_only ? 0 : P * (N + 1) * sizeof(float4)), 256);
+    L.filt = o;   o = align_up(o + S * sizeof(float), 256);
+    L.wS = o;     o = align_up(o + S * sizeof(float), 256);
+    L.wP = o;     o = align_up(o + P * sizeof(float), 256);
+    L.pulse = o;  o = align_up(o + P * sizeof(double4), 256);
+    L.tiles = o;  o = align_up(o + ntiles * sizeof(TileInfo), 256);
+    L.recs = o;   o = align_up(o + ntiles * P * sizeof(PulseRec), 256);
+    L.fin = o;    o = align_up(o + (tiles ? (size_t)j.nu * j.nv * sizeof(float2) : 0), 256);
     L.end = o;
     return L;
 }
@@ -164,7 +175,7 @@ cudaError_t DeviceInfo::record(int i, cudaStream_t st) {
 }
 
 void DeviceInfo::release() {
-    for (int i = 0; i < 5; ++i)
+    for (int i = 0; i < kEvents; ++i)
         if (ev[i]) cudaEventDestroy(ev[i]);
     for (auto &kv : twiddles) cudaFree(kv.second);
     twiddles.clear();
@@ -174,6 +185,7 @@ BpLaunch default_launch(const sarbp_opts *opts, int num_sms) {
     BpLaunch L;
     L.tile_x = 32;
     L.tile_y = 32;
+    L.minb = 3;
     L.stage_cap = 2048;
     L.cmax = 64;
     L.persistent = 1;
@@ -184,14 +196,18 @@ BpLaunch default_launch(const sarbp_opts *opts, int num_sms) {
         }
         if (opts->pulse_chunk > 0) L.cmax = std::min(256, std::max(4, opts->pulse_chunk));
         L.persistent = opts->persistent == 2 ? 0 : 1;
-        if (opts->stage_cap > 0) L.stage_cap = std::max(64, std::min(12288, opts->stage_cap));
+        if (opts->stage_cap > 0) L.stage_cap = std::max(64, std::min(4096, opts->stage_cap)) & ~1;
+        if (opts->min_blocks == 2 || opts->min_blocks == 3) L.minb = opts->min_blocks;
     }
     L.cmax = (L.cmax + 3) / 4 * 4;
     L.grid = num_sms;
     return L;
 }
 
-size_t Runner::job_scratch_bytes(const sarbp_job &j) { return layout_of(j, 0).end; }
+size_t Runner::job_scratch_bytes(const sarbp_job &j) {
+    const BpLaunch L = default_launch(nullptr, 148);
+    return layout_of(j, 0, L.tile_x, L.tile_y, false, j.precision == SARBP_PREC_NAIVE).end;
+}
 
 Runner::~Runner() {
     scratch_.release();
@@ -205,9 +221,10 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
     const bool rc_only = q_out != nullptr;
     if (njobs < 1 || !jobs) return fail(SARBP_ERR_INVALID, "no jobs");
     BpLaunch L = default_launch(opts, dev_->num_sms);
-    if (!bp_tile_supported(L.tile_x, L.tile_y))
+    if (!bp_tile_supported(L.tile_x, L.tile_y, L.minb))
         return fail(SARBP_ERR_INVALID, "unsupported pixel tile " + std::to_string(L.tile_x) + "x" +
-                                           std::to_string(L.tile_y));
+                                           std::to_string(L.tile_y) + " at " + std::to_string(L.minb) +
+                                           " CTAs/SM");
     std::vector<int> prec(njobs);
     for (int i = 0; i < njobs; ++i) {
         prec[i] = precision_of(jobs[i], opts);
@@ -222,7 +239,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
     size_t off = align_up((size_t)njobs * sizeof(JobScalars), 256);
     std::vector<JobLayout> lay(njobs);
     for (int i = 0; i < njobs; ++i) {
-        lay[i] = layout_of(jobs[i], off);
+        lay[i] = layout_of(jobs[i], off, L.tile_x, L.tile_y, rc_only, prec[i] == SARBP_PREC_NAIVE);
         off = lay[i].end;
     }
     cudaError_t e = scratch_.ensure(off, st);
@@ -304,6 +321,10 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
             dj.vh[k] = j.v_hat[k];
         }
         dj.Q = reinterpret_cast<float2 *>(sbase + lay[i].Q);
+        dj.Qp = rc_only ? nullptr : reinterpret_cast<float4 *>(sbase + lay[i].Qp);
+        dj.tiles = reinterpret_cast<TileInfo *>(sbase + lay[i].tiles);
+        dj.recs = reinterpret_cast<PulseRec *>(sbase + lay[i].recs);
+        dj.fin = reinterpret_cast<float2 *>(sbase + lay[i].fin);
         dj.filt = reinterpret_cast<float *>(sbase + lay[i].filt);
         dj.wS = reinterpret_cast<float *>(sbase + lay[i].wS);
         dj.wP = reinterpret_cast<float *>(sbase + lay[i].wP);
@@ -347,7 +368,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         e = dev_->twiddle(row_groups[g].first, &tw);
         if (e != cudaSuccess) return cuda_fail(e, "twiddle table");
     }
-    for (int k = 0; k < 5; ++k) dev_->ev_recorded[k] = false;
+    for (int k = 0; k < DeviceInfo::kEvents; ++k) dev_->ev_recorded[k] = false;
     if ((e = dev_->record(0, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
     launch_prep(d_jobs, njobs, st);
     dev_->launches++;
@@ -359,7 +380,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         float2 *tw = nullptr;
         e = dev_->twiddle(logN, &tw);
         if (e != cudaSuccess) return cuda_fail(e, "twiddle table");
-        e = launch_range_compress(logN, d_jobs, d_rows + first, (int)count, tw, st);
+        e = launch_range_compress(logN, d_jobs, d_rows + first, (int)count, rc_only ? 0 : 1, tw, st);
         if (e != cudaSuccess) return cuda_fail(e, "range compression launch");
         dev_->launches++;
     }
@@ -372,6 +393,16 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         last_status_dev_ = reinterpret_cast<int *>(sbase);
         return SARBP_OK;
     }
+    if (!items.empty()) {
+        int max_p = 0;
+        for (int i = 0; i < njobs; ++i)
+            if (prec[i] != SARBP_PREC_NAIVE) max_p = std::max(max_p, jobs[i].npulses);
+        e = launch_tile_setup(d_jobs, d_items, (int)items.size(), st);
+        if (e == cudaSuccess) e = launch_pulse_records(d_jobs, d_items, (int)items.size(), max_p, st);
+        if (e != cudaSuccess) return cuda_fail(e, "tile geometry launch");
+        dev_->launches += 2;
+    }
+    if ((e = dev_->record(3, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
     if (!items.empty()) {
         if (L.persistent) {
             const int occ = bp_max_active_blocks(L);
@@ -387,14 +418,14 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         if (e != cudaSuccess) return cuda_fail(e, "naive backprojection launch");
         dev_->launches++;
     }
-    if ((e = dev_->record(3, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    if ((e = dev_->record(4, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
     bool any_u8 = false;
     for (int i = 0; i < njobs; ++i) any_u8 = any_u8 || jobs[i].out_u8;
     if (any_u8) {
         e = launch_batch_u8(d_jobs, njobs, st);
         if (e != cudaSuccess) return cuda_fail(e, "u8 launch");
         dev_->launches++;
-        if ((e = dev_->record(4, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+        if ((e = dev_->record(5, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
     }
     last_njobs_ = njobs;
     last_status_dev_ = reinterpret_cast<int *>(sbase);
@@ -414,6 +445,9 @@ int Runner::check_status(cudaStream_t st) {
             return fail(SARBP_ERR_GEOMETRY, "job " + std::to_string(i) +
                                                 ": non-finite pixel or antenna position (those "
                                                 "pixels or pulses were left out)");
+        if (s & kStatusTimeout)
+            return fail(SARBP_ERR_TIMEOUT, "job " + std::to_string(i) +
+                                               ": a bounded wait for a range-profile copy gave up");
         if (s & kStatusTileTooWide)
             return fail(SARBP_ERR_GEOMETRY,
                         "job " + std::to_string(i) +

@@ -44,10 +44,12 @@ struct DeviceInfo {
     std::map<int, float2 *> twiddles;  // logN -> device table
     long long launches = 0;
     // stage timing: events [0] before set-up, [1] after set-up, [2] after
-    // range compression, [3] after backprojection, [4] after u8
+    // range compression, [3] after tile geometry, [4] after backprojection,
+    // [5] after u8
+    static constexpr int kEvents = 6;
     bool timing = false;
-    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-    bool ev_recorded[5] = {false, false, false, false, false};
+    cudaEvent_t ev[kEvents] = {};
+    bool ev_recorded[kEvents] = {};
     cudaError_t record(int i, cudaStream_t st);
     cudaError_t twiddle(int logN, float2 **out);
     void release();

@@ -88,7 +88,7 @@ def pixel_locs(u, v, u_hat, v_hat):
     return out
 
 
-def _opts(precision=None, tile=None, pulse_chunk=0, persistent=0, stage_cap=0):
+def _opts(precision=None, tile=None, pulse_chunk=0, persistent=0, stage_cap=0, min_blocks=0):
     o = Opts()
     o.precision = PREC_COMPAT if precision is None else int(precision)
     if tile:
@@ -96,6 +96,7 @@ def _opts(precision=None, tile=None, pulse_chunk=0, persistent=0, stage_cap=0):
     o.pulse_chunk = int(pulse_chunk)
     o.persistent = int(persistent)
     o.stage_cap = int(stage_cap)
+    o.min_blocks = int(min_blocks)
     return o
 
 
@@ -140,8 +141,9 @@ class Context:
         check(lib().sarbp_ctx_set_timing(self._h, int(bool(on))))
 
     def last_stage_ms(self):
-        """(set-up, range compression, backprojection, u8) ms of the last batch."""
-        ms = (ctypes.c_float * 4)()
+        """(set-up, range compression, tile geometry, backprojection, u8) ms
+        of the last batch."""
+        ms = (ctypes.c_float * 5)()
         check(lib().sarbp_ctx_last_stage_ms(self._h, ms))
         return tuple(float(x) for x in ms)
 

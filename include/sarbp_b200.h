@@ -62,8 +62,9 @@ typedef struct sarbp_opts {
     int tile_y;      /* pixel tile height (must give tile_x*tile_y in {256..4096}) */
     int pulse_chunk; /* pulses staged per chunk (4..256) */
     int persistent;  /* 0 or 1: persistent work-list launch; 2: one CTA per tile */
-    int stage_cap;   /* float4 entries of the range-window staging buffer */
-    int reserved[2];
+    int stage_cap;   /* float4 entries of each half of the range-window staging buffer */
+    int min_blocks;  /* CTAs per SM the kernel's registers are sized for (2 or 3) */
+    int reserved;
 } sarbp_opts;
 
 /*
@@ -103,9 +104,9 @@ long long sarbp_ctx_launch_count(sarbp_ctx *ctx);
 /* Record CUDA events around each stage of every batch (on = 1). */
 int sarbp_ctx_set_timing(sarbp_ctx *ctx, int on);
 /* Device time (ms) of the last batch's stages: [0] set-up kernel, [1] range
- * compression, [2] backprojection, [3] u8 output; -1 for a stage that did
- * not run.  Waits for the batch. */
-int sarbp_ctx_last_stage_ms(sarbp_ctx *ctx, float *ms4);
+ * compression, [2] tile geometry, [3] backprojection, [4] u8 output; -1 for
+ * a stage that did not run.  Waits for the batch. */
+int sarbp_ctx_last_stage_ms(sarbp_ctx *ctx, float *ms5);
 /* Measured FP32 FFMA instructions/s and SFU (MUFU) operations/s of the
  * context's device, from two chain microkernels. */
 int sarbp_measure_peaks(sarbp_ctx *ctx, double *ffma_per_s, double *mufu_per_s);

@@ -213,8 +213,12 @@ def test_ragged_sizes(ctx, oracle, P, S, nu, nv):
 
 def test_scattered_pixels(ctx, oracle, cfg1):
     """Pixel positions that are not a grid (a random shuffle of the plane):
-    each tile's window is wide, which the kernel must either handle exactly
-    or reject with an error code (never a wrong image)."""
+    each tile spans the whole 50 m scene, so the per-pixel offsets are tens
+    of metres and the closed-form range path keeps only f32 relative
+    precision on them (~|offset| * 6e-8 m, ~1e-3 rad of phase at X band).
+    Tolerance here: relative L2 <= 1e-3 -- or the call is rejected with
+    SARBP_ERR_GEOMETRY when a tile's range window exceeds the staging
+    buffer; never a silently wrong image."""
     d = cfg1
     rng = np.random.default_rng(5)
     n = 64
@@ -229,7 +233,7 @@ def test_scattered_pixels(ctx, oracle, cfg1):
         return
     ref = oracle.backprojection(d["phs"], k32, d["taylor"], d["N_fft"], d["delta_r"], pos32, r, n, n,
                                 mode=oracle.MODE_REF)
-    assert rel_l2(img, ref) < REL_COMPAT
+    assert rel_l2(img, ref) < 1e-3
 
 
 def test_batch_matches_single_bitwise(sb, ctx, torch):
@@ -337,4 +341,5 @@ def test_kernels_are_launched(ctx, cfg1):
     before = ctx.launch_count()
     ctx.backprojection_cuda(d["phs"], d["k_r"].astype(np.float32), d["taylor"], d["N_fft"], d["delta_r"],
                             d["u"], d["v"], d["pos"].astype(np.float32), d["r"])
-    assert ctx.launch_count() - before == 3  # prep, range compression, backprojection
+    # set-up, range compression, tile set-up, pulse records, backprojection
+    assert ctx.launch_count() - before == 5
