@@ -221,6 +221,8 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
     const bool rc_only = q_out != nullptr;
     if (njobs < 1 || !jobs) return fail(SARBP_ERR_INVALID, "no jobs");
     BpLaunch L = default_launch(opts, dev_->num_sms);
+    // a tile shape without a 3-CTA/SM build runs at 2 unless the caller asked
+    if (!bp_tile_supported(L.tile_x, L.tile_y, L.minb) && !(opts && opts->min_blocks)) L.minb = 2;
     if (!bp_tile_supported(L.tile_x, L.tile_y, L.minb))
         return fail(SARBP_ERR_INVALID, "unsupported pixel tile " + std::to_string(L.tile_x) + "x" +
                                            std::to_string(L.tile_y) + " at " + std::to_string(L.minb) +
