@@ -50,6 +50,30 @@ std::vector<double> taylor_coefficients(double S_L) {
     return F;
 }
 
+// signal.h:28-41 as above, for callers that may not allocate.
+int taylor_coefficients_into(double S_L, double *out, int cap) {
+    const float p10 = std::pow(10.0f, (float)(S_L * (1.0 / 20)));
+    const float acosh_f = std::log(p10 + std::sqrt(p10 * p10 - 1.0f));
+    const double A = (1.0 / kPi) * (double)acosh_f;
+    const double A2 = A * A;
+    const int n_bar = (int)(2 * A2 + 0.5) + 1;
+    const double nh = (double)n_bar - 0.5;
+    const double sp2 = ((double)n_bar / std::sqrt(A2 + nh * nh)) * ((double)n_bar / std::sqrt(A2 + nh * nh));
+    const int nr = n_bar - 1;
+    for (int m = 0; m < nr && m < cap; ++m) {
+        const long long m1sq = (long long)(m + 1) * (m + 1);
+        const float sgn = std::pow(-1.0f, (float)(m + 2));
+        double num = 1.0, den = 1.0;
+        for (int r = 0; r < nr; ++r) {
+            const double rh = (double)r + 0.5;
+            num = num * ((double)sgn * (1.0 - (double)m1sq / sp2 / (A2 + rh * rh)));
+            if (r != m) den = den * (1.0 - (double)div_floor(m1sq, (long long)(r + 1) * (r + 1)));
+        }
+        out[m] = num / den;
+    }
+    return nr > 0 ? nr : 0;
+}
+
 // signal.h:43-48: w(x) = 1 + sum_r F(r) cos(2 pi (r+1) xi), xi = linspace(-1/2, 1/2, num)
 void taylor_window(int num, double S_L, double *out) {
     const std::vector<double> F = taylor_coefficients(S_L);

@@ -8,6 +8,9 @@ namespace sarbp {
 // Taylor window coefficients F_m (signal.h:28-41) for side-lobe level S_L;
 // returns n_bar - 1 values.
 std::vector<double> taylor_coefficients(double S_L);
+// The same coefficients written into out[0..cap) without allocating; returns
+// their count (n_bar - 1), which may exceed cap (then only cap are written).
+int taylor_coefficients_into(double S_L, double *out, int cap);
 // Full Taylor window (signal.h:14-51), normalised to its maximum.
 void taylor_window(int num, double S_L, double *out);
 

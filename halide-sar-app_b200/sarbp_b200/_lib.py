@@ -80,6 +80,7 @@ SIGNATURES = {
                                           ctypes.POINTER(Opts)]),
     "sarbp_range_compress_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job),
                                                    ctypes.POINTER(Opts), _dp]),
+    "sarbp_backprojection_noalloc": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.c_void_p, _dp]),
     "sarbp_img_output_to_dB": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, _dp]),
     "sarbp_img_output_u8": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_double, ctypes.c_double, _dp]),

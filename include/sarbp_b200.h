@@ -157,6 +157,27 @@ int sarbp_range_compress_device(sarbp_ctx *ctx, const sarbp_job *job,
 int sarbp_batch_device(sarbp_ctx *ctx, const sarbp_job *jobs, int njobs,
                        const sarbp_opts *opts);
 
+/*
+ * Backprojection of one device-resident job that allocates nothing (no
+ * counterpart in the reference).  For callers that cannot allocate device
+ * memory when they need an image -- inside a stream capture, under a memory
+ * pool they do not own, or in a loop that must not touch the allocator.
+ * Runs the same kernels as sarbp_backprojection_device on `cuda_stream`,
+ * with all scratch in one static 64 MiB device array of the library:
+ *  - jobs needing more scratch than that return SARBP_ERR_UNSUPPORTED
+ *    (roughly: 16 B x npulses x n_fft + 32 B x npulses x tiles of 32x32
+ *    pixels + 8 B x pixels);
+ *  - every call shares the array, so calls must not overlap on the GPU;
+ *  - the first call on a device looks up the array and sets kernel
+ *    attributes -- make it before any stream capture;
+ *  - precision SARBP_PREC_COMPAT or SARBP_PREC_PRECISE only;
+ *  - `status` (device int, may be NULL) receives the kernels' status bits
+ *    (0 = fine; 1 = a pixel tile too spread out; 2 = non-finite geometry;
+ *    8 = a bounded wait for a copy gave up).
+ * The array stays allocated on every GPU that loads the library until exit.
+ */
+int sarbp_backprojection_noalloc(const sarbp_job *job, void *cuda_stream, int *status);
+
 /* ---- dB / u8 output stages (img_output.cpp:10-52) ---- */
 /* dB = 10*log10(|z| / max|z|) for a complex128 [nv][nu] image. */
 int sarbp_img_output_to_dB(sarbp_ctx *ctx, const double *img, int nu, int nv,
