@@ -38,6 +38,9 @@ sys.path.insert(0, os.path.join(ROOT, "halide-sar-app_b200"))
 
 FP32_PER_UNIT = 18  # FP32-pipe instructions per pixel*pulse (algorithmic)
 SFU_PER_UNIT = 3    # SFU operations per pixel*pulse (algorithmic)
+# DRAM bytes (read + write) of one bp_tile_kernel launch, from an ncu capture
+# of the default plain_large step (profiles/bp_tile_kernel_32x32_plain_large_2048x1999.md)
+NCU_BP_TRAFFIC = {"plain_large": 571.617024e6 + 82.065408e6}
 
 
 def parse():
@@ -246,6 +249,7 @@ def run_ours(args, rank, world, local_rank):
         tune["stage_cap"] = args.stage_cap
     if args.min_blocks:
         tune["min_blocks"] = args.min_blocks
+    default_launch = not tune
     job = sb.make_job(S, P, data["N_fft"], data["taylor"], nu, nv, data["delta_r"], t_phs.data_ptr(),
                       t_k.data_ptr(), t_pos.data_ptr(), t_out.data_ptr(), r=t_r.data_ptr())
 
@@ -367,7 +371,8 @@ def run_ours(args, rank, world, local_rank):
         "stage_ms": {"setup": prep_ms, "range_compress": rc_ms, "tile_geometry": geom_ms, "backproject": bp_ms,
                      "db_u8": float(np.mean(u8_ms))},
         "roofline": {"bound": bound, "achieved": achieved, "peak": peak, "unit": "Tops/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak,
+                     "traffic": NCU_BP_TRAFFIC.get(args.config) if default_launch else None,
                      "kernel": "bp_tile_kernel",
                      "per_unit": "%d FP32 instr + %d SFU ops per pixel*pulse" % (FP32_PER_UNIT, SFU_PER_UNIT),
                      "peak_source": "measured in this run: FFMA / MUFU chain microkernels",

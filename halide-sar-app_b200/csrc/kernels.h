@@ -54,6 +54,6 @@ cudaError_t launch_db_u8(const double2 *img, long long n, const unsigned long lo
 cudaError_t launch_u8_from_db(const double *dB, long long n, double dB_min, double dB_max,
                               uint8_t *u8, cudaStream_t st);
 // u8 images of every job of a batch that asked for one (uses DevJob::maxabs)
-cudaError_t launch_batch_u8(const DevJob *d_jobs, int njobs, cudaStream_t st);
+cudaError_t launch_batch_u8(const DevJob *d_jobs, int njobs, long long max_pixels, cudaStream_t st);
 
 }  // namespace sarbp

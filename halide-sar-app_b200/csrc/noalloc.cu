@@ -238,7 +238,7 @@ extern "C" int sarbp_backprojection_noalloc(const sarbp_job *job, void *cuda_str
     if (occ < 1) return fail(SARBP_ERR_CUDA, "no-alloc: backprojection kernel does not fit on an SM");
     L.grid = (int)std::min<long long>((long long)occ * num_sms, (long long)ntiles);
     e = launch_backproject(L, d_job, d_items, (int)ntiles, d_cnt, st);
-    if (e == cudaSuccess && j.out_u8) e = launch_batch_u8(d_job, 1, st);
+    if (e == cudaSuccess && j.out_u8) e = launch_batch_u8(d_job, 1, (long long)j.nu * j.nv, st);
     if (e == cudaSuccess && status) {
         status_kernel<<<1, 1, 0, st>>>(dj.sc, status);
         e = cudaGetLastError();

@@ -8,6 +8,9 @@
 // All HBM-bound; the fused form reads the complex image once and writes the
 // u8 (and optionally the f64 dB) image, using the max|z| that the
 // backprojection epilogue already reduced.
+#include <algorithm>
+#include <cstdint>
+
 #include "internal.h"
 #include "kernels.h"
 
@@ -64,17 +67,35 @@ __global__ void u8_from_db_kernel(const double *__restrict__ dB, long long n, do
         u8[i] = to_u8(dB[i], lo, hi);
 }
 
-// blockIdx.y = job; jobs without an u8 output return at once
+// blockIdx.y = job; jobs without an u8 output return at once.  Each thread
+// converts four neighbouring pixels (64 B of complex f64 in, one 32-bit word
+// of u8 out when the destination is 4-byte aligned).
 __global__ void batch_u8_kernel(const DevJob *__restrict__ jobs) {
     const DevJob &jb = jobs[blockIdx.y];
     if (!jb.out_u8) return;
     const double m = __longlong_as_double((long long)jb.sc->maxabs);
     const long long n = (long long)jb.nu * jb.nv;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
-        const double2 z = jb.out[i];
-        const double a = sqrt(z.x * z.x + z.y * z.y);
-        jb.out_u8[i] = to_u8(10.0 * (log(a / m) / kLn10F32), jb.dB_min, jb.dB_max);
+    const double lo = jb.dB_min, hi = jb.dB_max;
+    const bool vec = ((reinterpret_cast<uintptr_t>(jb.out_u8) & 3) == 0);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; 4 * q < n; q += stride) {
+        const long long i0 = 4 * q;
+        if (vec && i0 + 4 <= n) {
+            uint32_t w = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const double2 z = jb.out[i0 + k];
+                const double a = sqrt(z.x * z.x + z.y * z.y);
+                w |= (uint32_t)to_u8(10.0 * (log(a / m) / kLn10F32), lo, hi) << (8 * k);
+            }
+            *reinterpret_cast<uint32_t *>(jb.out_u8 + i0) = w;
+        } else {
+            for (long long i = i0; i < n && i < i0 + 4; ++i) {
+                const double2 z = jb.out[i];
+                const double a = sqrt(z.x * z.x + z.y * z.y);
+                jb.out_u8[i] = to_u8(10.0 * (log(a / m) / kLn10F32), lo, hi);
+            }
+        }
     }
 }
 
@@ -104,8 +125,12 @@ cudaError_t launch_u8_from_db(const double *dB, long long n, double lo, double h
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch_u8(const DevJob *d_jobs, int njobs, cudaStream_t st) {
-    batch_u8_kernel<<<dim3(64, njobs), 256, 0, st>>>(d_jobs);
+cudaError_t launch_batch_u8(const DevJob *d_jobs, int njobs, long long max_pixels, cudaStream_t st) {
+    // about eight 256-thread blocks per SM over the whole batch
+    long long bx = (max_pixels / 4 + 255) / 256;
+    const long long cap = std::max<long long>(1, (148LL * 8 + njobs - 1) / njobs);
+    bx = std::max<long long>(1, std::min(bx, cap));
+    batch_u8_kernel<<<dim3((unsigned)bx, njobs), 256, 0, st>>>(d_jobs);
     return cudaGetLastError();
 }
 

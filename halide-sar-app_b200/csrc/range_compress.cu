@@ -42,43 +42,38 @@ __device__ __forceinline__ float2 w16(int j) {
     }
 }
 
-__host__ __device__ constexpr int bitrev(int i, int bits) {
-    int r = 0;
-    for (int b = 0; b < bits; ++b) r |= ((i >> b) & 1) << (bits - 1 - b);
-    return r;
-}
 __host__ __device__ constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n >> 1); }
 
-// In-register forward DFT of R points v[B..B+R), natural order in and out
-// (radix-2 decimation in time on a bit-reversed copy).
+// In-register forward DFT of R points v[B..B+R), natural order in and out:
+// log2(R) self-sorting (Stockham) radix-2 stages, every index an affine
+// function of unrolled loop counters so the values stay in registers.
 template <int R, int B>
 __device__ __forceinline__ void dft_reg(float2 (&v)[16]) {
-    constexpr int L = ilog2(R);
-    float2 a[R];
+    float2 x[R], y[R];
 #pragma unroll
-    for (int i = 0; i < R; ++i) a[i] = v[B + bitrev(i, L)];
+    for (int i = 0; i < R; ++i) x[i] = v[B + i];
 #pragma unroll
-    for (int len = 2; len <= R; len <<= 1) {
-        const int half = len >> 1;
+    for (int ns = 1; ns < R; ns <<= 1) {
 #pragma unroll
-        for (int i = 0; i < R; i += len) {
-#pragma unroll
-            for (int k = 0; k < half; ++k) {
-                const int j = k * (16 / len);  // W_len^k = W_16^(k*16/len)
-                float2 t = a[i + k + half];
-                if (j == 4) {
-                    t = make_float2(t.y, -t.x);  // * (-i)
-                } else if (j != 0) {
-                    t = cmul(t, w16(j));
-                }
-                const float2 u = a[i + k];
-                a[i + k] = make_float2(u.x + t.x, u.y + t.y);
-                a[i + k + half] = make_float2(u.x - t.x, u.y - t.y);
+        for (int j = 0; j < R / 2; ++j) {
+            const int k = j & (ns - 1);
+            const int tw = k * (8 / ns);  // W_{2ns}^k = W_16^(8k/ns)
+            const float2 a = x[j];
+            float2 b = x[j + R / 2];
+            if (tw == 4) {
+                b = make_float2(b.y, -b.x);  // * (-i)
+            } else if (tw != 0) {
+                b = cmul(b, w16(tw));
             }
+            const int o = (j / ns) * 2 * ns + k;
+            y[o] = make_float2(a.x + b.x, a.y + b.y);
+            y[o + ns] = make_float2(a.x - b.x, a.y - b.y);
         }
+#pragma unroll
+        for (int i = 0; i < R; ++i) x[i] = y[i];
     }
 #pragma unroll
-    for (int i = 0; i < R; ++i) v[B + i] = a[i];
+    for (int i = 0; i < R; ++i) v[B + i] = x[i];
 }
 
 __device__ __forceinline__ int pad_idx(int i) { return i + (i >> 4); }
@@ -141,7 +136,6 @@ template <int N>
 struct Plan {
     static constexpr int L = ilog2(N);
     static constexpr int R0 = 1 << (L % 4);  // 1 means no leading pass
-    static constexpr int NP16 = L / 4;
 };
 
 // Recursive radix-16 passes; pass index K has NS = R0 * 16^K.  The last

@@ -422,9 +422,13 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
     }
     if ((e = dev_->record(4, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
     bool any_u8 = false;
-    for (int i = 0; i < njobs; ++i) any_u8 = any_u8 || jobs[i].out_u8;
+    long long max_px = 0;
+    for (int i = 0; i < njobs; ++i) {
+        any_u8 = any_u8 || jobs[i].out_u8;
+        max_px = std::max(max_px, (long long)jobs[i].nu * jobs[i].nv);
+    }
     if (any_u8) {
-        e = launch_batch_u8(d_jobs, njobs, st);
+        e = launch_batch_u8(d_jobs, njobs, max_px, st);
         if (e != cudaSuccess) return cuda_fail(e, "u8 launch");
         dev_->launches++;
         if ((e = dev_->record(5, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
