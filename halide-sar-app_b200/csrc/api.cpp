@@ -39,13 +39,21 @@ int set_device(sarbp_ctx *ctx) {
 }
 
 // Copies host arrays to one device block, runs one job, copies the image back.
+// An image plane given by its axes instead of pixel_locs: pixel (i, j) sits
+// at u_hat * u[i] + v_hat * v[j] (img_plane.cpp:92-102), formed on the device.
+struct PlaneAxes {
+    const double *u, *v, *u_hat, *v_hat;
+};
+
 int run_host_job(sarbp_ctx *ctx, const float *phs, int S, int P, const float *k_r32,
                  const double *k_r64, int taylor, int n_fft, double delta_r, int nu, int nv,
                  const float *pos32, const double *pos64, const double *r, double *out,
-                 const sarbp_opts *opts, int precision) {
+                 const sarbp_opts *opts, int precision, const PlaneAxes *plane = nullptr) {
     int rc = set_device(ctx);
     if (rc) return rc;
-    if (!phs || !r || !out) return fail(SARBP_ERR_INVALID, "phs, r and output_img must be non-NULL");
+    if (!phs || !out) return fail(SARBP_ERR_INVALID, "phs and output_img must be non-NULL");
+    if (!r && !(plane && plane->u && plane->v && plane->u_hat && plane->v_hat))
+        return fail(SARBP_ERR_INVALID, "r (pixel_locs) must be non-NULL");
     if (S < 1 || P < 1 || nu < 1 || nv < 1) return fail(SARBP_ERR_INVALID, "sizes must be >= 1");
     const size_t npix = (size_t)nu * nv;
     const size_t b_phs = align256((size_t)S * P * 2 * sizeof(float));
@@ -53,9 +61,11 @@ int run_host_job(sarbp_ctx *ctx, const float *phs, int S, int P, const float *k_
     const size_t b_k64 = k_r64 ? align256((size_t)S * sizeof(double)) : 0;
     const size_t b_p32 = pos32 ? align256((size_t)P * 3 * sizeof(float)) : 0;
     const size_t b_p64 = pos64 ? align256((size_t)P * 3 * sizeof(double)) : 0;
-    const size_t b_r = align256(npix * 3 * sizeof(double));
+    const size_t b_r = r ? align256(npix * 3 * sizeof(double)) : 0;
+    const size_t b_u = r ? 0 : align256((size_t)nu * sizeof(double));
+    const size_t b_v = r ? 0 : align256((size_t)nv * sizeof(double));
     const size_t b_out = align256(npix * 2 * sizeof(double));
-    const size_t total = b_phs + b_k32 + b_k64 + b_p32 + b_p64 + b_r + b_out;
+    const size_t total = b_phs + b_k32 + b_k64 + b_p32 + b_p64 + b_r + b_u + b_v + b_out;
     cudaError_t e = ctx->io.ensure(total, ctx->stream);
     if (e != cudaSuccess) return cuda_fail(e, "allocating device inputs");
     char *base = static_cast<char *>(ctx->io.ptr);
@@ -65,7 +75,9 @@ int run_host_job(sarbp_ctx *ctx, const float *phs, int S, int P, const float *k_
     double *d_k64 = k_r64 ? reinterpret_cast<double *>(base + o) : nullptr; o += b_k64;
     float *d_p32 = pos32 ? reinterpret_cast<float *>(base + o) : nullptr; o += b_p32;
     double *d_p64 = pos64 ? reinterpret_cast<double *>(base + o) : nullptr; o += b_p64;
-    double *d_r = reinterpret_cast<double *>(base + o); o += b_r;
+    double *d_r = r ? reinterpret_cast<double *>(base + o) : nullptr; o += b_r;
+    double *d_u = r ? nullptr : reinterpret_cast<double *>(base + o); o += b_u;
+    double *d_v = r ? nullptr : reinterpret_cast<double *>(base + o); o += b_v;
     double *d_out = reinterpret_cast<double *>(base + o);
     cudaStream_t st = ctx->stream;
     struct Copy { void *dst; const void *src; size_t n; };
@@ -76,6 +88,8 @@ int run_host_job(sarbp_ctx *ctx, const float *phs, int S, int P, const float *k_
         {d_p32, pos32, (size_t)P * 3 * sizeof(float)},
         {d_p64, pos64, (size_t)P * 3 * sizeof(double)},
         {d_r, r, npix * 3 * sizeof(double)},
+        {d_u, r ? nullptr : plane->u, (size_t)nu * sizeof(double)},
+        {d_v, r ? nullptr : plane->v, (size_t)nv * sizeof(double)},
     };
     for (const Copy &c : copies) {
         if (!c.src) continue;
@@ -97,6 +111,14 @@ int run_host_job(sarbp_ctx *ctx, const float *phs, int S, int P, const float *k_
     j.pos = d_p32;
     j.pos64 = d_p64;
     j.r = d_r;
+    if (!r) {
+        j.u = d_u;
+        j.v = d_v;
+        for (int d = 0; d < 3; ++d) {
+            j.u_hat[d] = plane->u_hat[d];
+            j.v_hat[d] = plane->v_hat[d];
+        }
+    }
     j.output_img = d_out;
     j.precision = precision;
     rc = ctx->runner->enqueue(&j, 1, opts, st);
@@ -229,6 +251,20 @@ int sarbp_backprojection(sarbp_ctx *ctx, const float *phs, int nsamples, int npu
     return run_host_job(ctx, phs, nsamples, npulses, k_r, nullptr, taylor_s_l, n_fft, delta_r, nu,
                         nv, pos, nullptr, r, output_img, opts,
                         effective_precision(opts, SARBP_PREC_COMPAT));
+}
+
+int sarbp_backprojection_plane(sarbp_ctx *ctx, const float *phs, int nsamples, int npulses,
+                               const float *k_r, int taylor_s_l, int n_fft, double delta_r,
+                               const double *u, int nu, const double *v, int nv,
+                               const double u_hat[3], const double v_hat[3], const float *pos,
+                               double *output_img, const sarbp_opts *opts) {
+    if (!k_r || !pos) return fail(SARBP_ERR_INVALID, "k_r and pos must be non-NULL");
+    if (!u || !v || !u_hat || !v_hat)
+        return fail(SARBP_ERR_INVALID, "u, v, u_hat and v_hat must be non-NULL");
+    const PlaneAxes plane{u, v, u_hat, v_hat};
+    return run_host_job(ctx, phs, nsamples, npulses, k_r, nullptr, taylor_s_l, n_fft, delta_r, nu,
+                        nv, pos, nullptr, nullptr, output_img, opts,
+                        effective_precision(opts, SARBP_PREC_COMPAT), &plane);
 }
 
 int sarbp_backprojection_f64(sarbp_ctx *ctx, const float *phs, int nsamples, int npulses,

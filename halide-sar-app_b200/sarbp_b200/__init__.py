@@ -186,6 +186,28 @@ class Context:
                  _ptr(u), nu, _ptr(v), nv, _ptr(pos), _ptr(r), _ptr(out), ctypes.byref(o)))
         return out
 
+    def backprojection_plane(self, phs, k_r, taylor_s_l, N_fft, delta_r, u, v, u_hat, v_hat, pos,
+                             precision=None, **tune):
+        """backprojection_cuda with pixel_locs given by the image-plane axes:
+        pixel (i, j) = u_hat * u[i] + v_hat * v[j], formed on the device."""
+        phs = np.ascontiguousarray(phs, np.complex64)
+        P, S = phs.shape
+        u = np.ascontiguousarray(u, np.float64)
+        v = np.ascontiguousarray(v, np.float64)
+        uh = np.ascontiguousarray(u_hat, np.float64)
+        vh = np.ascontiguousarray(v_hat, np.float64)
+        pos = np.ascontiguousarray(pos, np.float32)
+        k_r = np.ascontiguousarray(k_r, np.float32)
+        if pos.size != 3 * P or k_r.size != S or uh.size != 3 or vh.size != 3:
+            raise SarbpError(ERR_INVALID, "pos must be [P, 3], k_r [S], u_hat and v_hat [3]")
+        nu, nv = u.size, v.size
+        out = np.empty((nv, nu), np.complex128)
+        o = _opts(PREC_COMPAT if precision is None else precision, **tune)
+        check(lib().sarbp_backprojection_plane(
+            self._h, _ptr(phs), S, P, _ptr(k_r), int(taylor_s_l), int(N_fft), float(delta_r),
+            _ptr(u), nu, _ptr(v), nv, _ptr(uh), _ptr(vh), _ptr(pos), _ptr(out), ctypes.byref(o)))
+        return out
+
     def img_output_to_dB(self, img):
         img = np.ascontiguousarray(img, np.complex128)
         nv, nu = img.shape

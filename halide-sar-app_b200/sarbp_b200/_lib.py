@@ -70,6 +70,10 @@ SIGNATURES = {
         ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
         ctypes.c_double, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp,
         ctypes.POINTER(Opts)]),
+    "sarbp_backprojection_plane": (ctypes.c_int, [
+        ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
+        ctypes.c_double, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp, _dp,
+        ctypes.POINTER(Opts)]),
     "sarbp_backprojection_f64": (ctypes.c_int, [
         ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
         ctypes.c_double, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp,

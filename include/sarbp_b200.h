@@ -127,6 +127,21 @@ int sarbp_backprojection(sarbp_ctx *ctx, const float *phs, int nsamples,
                          const double *r, double *output_img,
                          const sarbp_opts *opts);
 
+/*
+ * The same image from the image-plane axes instead of pixel_locs: pixel
+ * (i, j) is u_hat * u[i] + v_hat * v[j] (img_plane.cpp:92-102, the r array
+ * img_plane_create builds, ImgPlane.cpp:16-63), formed on the device in the
+ * same f64 arithmetic, so the nu*nv*3 f64 positions are neither built on the
+ * host nor copied.  Used by the sarbp CLI.
+ */
+int sarbp_backprojection_plane(sarbp_ctx *ctx, const float *phs, int nsamples,
+                               int npulses, const float *k_r, int taylor_s_l,
+                               int n_fft, double delta_r, const double *u,
+                               int nu, const double *v, int nv,
+                               const double u_hat[3], const double v_hat[3],
+                               const float *pos, double *output_img,
+                               const sarbp_opts *opts);
+
 /* The same with f64 positions and k_r (SARBP_PREC_PRECISE by default). */
 int sarbp_backprojection_f64(sarbp_ctx *ctx, const float *phs, int nsamples,
                              int npulses, const double *k_r, int taylor_s_l,
