@@ -7,6 +7,7 @@
 #include <string>
 #include <vector>
 
+#include "context.h"
 #include "host_math.h"
 #include "kernels.h"
 #include "runner.h"
@@ -18,33 +19,26 @@ const char *last_error_cstr();
 
 using namespace sarbp;
 
-struct sarbp_ctx {
-    DeviceInfo dev;
-    std::unique_ptr<Runner> runner;
-    cudaStream_t own_stream = nullptr;
-    cudaStream_t stream = nullptr;
-    DeviceBuffer io;  // device copies of host-API inputs and outputs
-    DeviceBuffer out_aux;
-};
-
-namespace {
-
-size_t align256(size_t x) { return (x + 255) / 256 * 256; }
-
-int set_device(sarbp_ctx *ctx) {
+int sarbp::ctx_set_device(sarbp_ctx *ctx) {
     if (!ctx) return fail(SARBP_ERR_INVALID, "context is NULL");
     cudaError_t e = cudaSetDevice(ctx->dev.device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
     return SARBP_OK;
 }
 
-// Copies host arrays to one device block, runs one job, copies the image back.
+namespace {
+
+size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+int set_device(sarbp_ctx *ctx) { return ctx_set_device(ctx); }
+
 // An image plane given by its axes instead of pixel_locs: pixel (i, j) sits
 // at u_hat * u[i] + v_hat * v[j] (img_plane.cpp:92-102), formed on the device.
 struct PlaneAxes {
     const double *u, *v, *u_hat, *v_hat;
 };
 
+// Copies host arrays to one device block, runs one job, copies the image back.
 int run_host_job(sarbp_ctx *ctx, const float *phs, int S, int P, const float *k_r32,
                  const double *k_r64, int taylor, int n_fft, double delta_r, int nu, int nv,
                  const float *pos32, const double *pos64, const double *r, double *out,

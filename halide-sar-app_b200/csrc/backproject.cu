@@ -13,9 +13,10 @@
 //     Delta = s + e t     (= k_c (R - |pos - r|) up to k_c rho^3/(2R^2))
 //     phase = theta + Delta,  range bin = t_c + Delta / (k_c lsr)
 // A chunk whose pulses are close enough for that truncation to exceed the
-// phase budget adds the next term, s + e t (1 + 2 e s); closer still, the
-// closed form 2R'h / (R' + sqrt(R'(R' - 2h))), R' = k_c R, h = s - e|d|^2,
-// is used.  |Delta| <= k_c rho, so each pulse only touches W = 2K+1 range
+// phase budget adds terms of the series in h = s - e|d|^2 (three or four);
+// in the near field the closed form 2R'h / (R' + sqrt(R'(R' - 2h))),
+// R' = k_c R, is used.  Tiles wider than kWideRad radians take the linear
+// phase toward a reference direction out of the loop (see accumulate).  |Delta| <= k_c rho, so each pulse only touches W = 2K+1 range
 // bins; range compression stored every bin as the pair
 //     (m, d) = ((Q[k] + Q[k+1]) / 2, Q[k+1] - Q[k])
 // so the reference's clamped lerp Q[l](1-w) + Q[l+1]w is m + (w-1/2) d: one
@@ -98,37 +99,58 @@ __device__ __forceinline__ void bulk_copy(void *dst, const void *src, uint32_t b
 }
 
 // Inner loop over the nc pulses of a chunk for a consumer's PPT pixels.
-// MODE 0: Delta = s + e t; 1: s + e t (1 + 2 e s); 2: closed form.
+// With h = s - e|d|^2 and y = e h, the exact range difference is the series
+//     Delta = h (1 + y + 2y^2 + 5y^3 + 14y^4 + ...)   (Catalan numbers)
+// MODE 0: Delta = s + e t, t = s^2 - |d|^2 (two terms);
+// MODE 1: s + e t (1 + 2 e s) (three terms);
+// MODE 2: h + h y (1 + 2y + 5y^2) (four terms), all FMA-pipe arithmetic;
+// MODE 3: the closed form 2R'h / (R' + sqrt(R'(R' - 2h))) (near field).
+// Modes 2 and 3 form the nonlinear part N = Delta - s on its own (mode 3 as
+// (s Delta - |d|^2) / (R' + r), free of the cancellation in Delta - s), so
+// their approximate divisions only see a small quantity.
 // PLANAR: every pixel of the tile has dz == 0.
-template <int MODE, bool PLANAR, int PPT>
+// WIDE: the records hold w_hat - w0, so the product with d is the small
+// sd = s - s0 (s0 = w0 . d per pixel); the phase is theta + sd + N with
+// every term small, and only the range bin uses the full s0 + ...:
+// exp(-j s0) is applied in f64 through the final phase.
+template <int MODE, bool PLANAR, bool WIDE, int PPT>
 __device__ __forceinline__ void accumulate(int nc, const PulseRec *__restrict__ rec, uint32_t poff,
                                            uint32_t pstride, float ilk, float hi_clamp,
                                            const float (&dx)[PPT], const float (&dy)[PPT],
-                                           const float (&dz)[PPT], const float (&nd2)[PPT], float (&ar)[PPT],
-                                           float (&ai)[PPT]) {
+                                           const float (&dz)[PPT], const float (&nd2)[PPT],
+                                           const float (&s0)[PPT], float (&ar)[PPT], float (&ai)[PPT]) {
 #pragma unroll 2
     for (int i = 0; i < nc; ++i, poff += pstride) {
-        const float4 a = rec[i].a;  // w_hat, e
+        const float4 a = rec[i].a;  // w_hat (or w_hat - w0), e
         const float4 b = rec[i].b;  // c0, theta, R', bits
         const float e2 = a.w + a.w;
 #pragma unroll
         for (int k = 0; k < PPT; ++k) {
-            float s = fmaf(a.y, dy[k], a.x * dx[k]);
-            if constexpr (!PLANAR) s = fmaf(a.z, dz[k], s);
-            float D;
+            float sd = fmaf(a.y, dy[k], a.x * dx[k]);
+            if constexpr (!PLANAR) sd = fmaf(a.z, dz[k], sd);
+            const float s = WIDE ? s0[k] + sd : sd;
+            float D;  // phase argument
             if constexpr (MODE == 0) {
-                D = fmaf(a.w, fmaf(s, s, nd2[k]), s) + b.y;
+                D = fmaf(a.w, fmaf(s, s, nd2[k]), sd) + b.y;
             } else if constexpr (MODE == 1) {
                 const float t = fmaf(s, s, nd2[k]);
-                D = fmaf(a.w * t, fmaf(e2, s, 1.0f), s) + b.y;
+                D = fmaf(a.w * t, fmaf(e2, s, 1.0f), sd) + b.y;
+            } else if constexpr (MODE == 2) {
+                const float en = a.w * nd2[k];  // h - s
+                const float h = s + en;
+                const float y = a.w * h;
+                const float q = fmaf(y, fmaf(5.0f, y, 2.0f), 1.0f);
+                D = (sd + fmaf(h * y, q, en)) + b.y;
             } else {
                 const float h = fmaf(a.w, nd2[k], s);
                 const float q = fmaxf(fmaf(-2.0f, h, b.z), 0.0f);
-                const float r = sqrtf(b.z * q);
-                D = (2.0f * b.z * h) / (b.z + r) + b.y;
+                const float den = b.z + sqrtf(b.z * q);
+                const float Dn = __fdividef(2.0f * b.z * h, den);
+                D = (sd + __fdividef(fmaf(s, Dn, nd2[k]), den)) + b.y;
             }
-            float tl = fmaf(D, ilk, b.x);
-            if constexpr (MODE == 2) tl = fminf(fmaxf(tl, 0.0f), hi_clamp);
+            const float Di = WIDE ? s0[k] + D : D;  // range-bin argument
+            float tl = fmaf(Di, ilk, b.x);
+            if constexpr (MODE >= 2) tl = fminf(fmaxf(tl, 0.0f), hi_clamp);
             const float f = tl + kMagic;
             const float wgt = tl - (f - kMagic);
             const uint32_t o = (__float_as_uint(f) << 4) + poff;  // shared-window address
@@ -146,21 +168,26 @@ __device__ __forceinline__ void accumulate(int nc, const PulseRec *__restrict__ 
     }
 }
 
-template <int PPT>
-__device__ __forceinline__ void accumulate_any(int mode, bool planar, int nc, const PulseRec *rec,
-                                               uint32_t poff, uint32_t pstride, float ilk, float hi,
-                                               const float (&dx)[PPT], const float (&dy)[PPT],
-                                               const float (&dz)[PPT], const float (&nd2)[PPT],
-                                               float (&ar)[PPT], float (&ai)[PPT]) {
+template <bool WIDE, int PPT>
+__device__ __forceinline__ void accumulate_mode(int mode, bool planar, int nc, const PulseRec *rec,
+                                                uint32_t poff, uint32_t pstride, float ilk, float hi,
+                                                const float (&dx)[PPT], const float (&dy)[PPT],
+                                                const float (&dz)[PPT], const float (&nd2)[PPT],
+                                                const float (&s0)[PPT], float (&ar)[PPT], float (&ai)[PPT]) {
+#define SARBP_ACC(M, PL) accumulate<M, PL, WIDE, PPT>(nc, rec, poff, pstride, ilk, hi, dx, dy, dz, nd2, s0, ar, ai)
     if (mode == 0) {
-        if (planar) accumulate<0, true, PPT>(nc, rec, poff, pstride, ilk, hi, dx, dy, dz, nd2, ar, ai);
-        else accumulate<0, false, PPT>(nc, rec, poff, pstride, ilk, hi, dx, dy, dz, nd2, ar, ai);
+        if (planar) SARBP_ACC(0, true);
+        else SARBP_ACC(0, false);
     } else if (mode == 1) {
-        if (planar) accumulate<1, true, PPT>(nc, rec, poff, pstride, ilk, hi, dx, dy, dz, nd2, ar, ai);
-        else accumulate<1, false, PPT>(nc, rec, poff, pstride, ilk, hi, dx, dy, dz, nd2, ar, ai);
+        if (planar) SARBP_ACC(1, true);
+        else SARBP_ACC(1, false);
+    } else if (mode == 2) {
+        if (planar) SARBP_ACC(2, true);
+        else SARBP_ACC(2, false);
     } else {
-        accumulate<2, false, PPT>(nc, rec, poff, pstride, ilk, hi, dx, dy, dz, nd2, ar, ai);
+        SARBP_ACC(3, false);
     }
+#undef SARBP_ACC
 }
 
 // Shared memory of the tile kernel.
@@ -211,8 +238,8 @@ __device__ __forceinline__ bool stage_chunk(const DevJob &jb, int tile, int lane
     int mode = 0;
     for (int i = lane; i < nc; i += 32) {
         const int bits = __float_as_int(rec[i].b.w);
-        const int base = bits >> 2, order = bits & 3;
-        if (order == 3) continue;  // invalid pulse: window stays zero
+        const int base = bits >> 3, order = bits & 7;
+        if (order == kOrderInvalid) continue;  // invalid pulse: window stays zero
         mode = max(mode, order);
         const int lo = max(base, 0), hi = min(base + W, N);
         if (hi > lo) bytes += (uint32_t)(hi - lo) * 16u;
@@ -228,10 +255,10 @@ __device__ __forceinline__ bool stage_chunk(const DevJob &jb, int tile, int lane
     __syncwarp();
     for (int i = lane; i < nc; i += 32) {
         const int bits = __float_as_int(rec[i].b.w);
-        const int base = bits >> 2, order = bits & 3;
+        const int base = bits >> 3, order = bits & 7;
         const float4 *row = jb.Qp + (size_t)(p0 + i) * (N + 1);
         float4 *dst = win + i * W;
-        if (order == 3) {
+        if (order == kOrderInvalid) {
             for (int j = 0; j < W; ++j) dst[j] = make_float4(0.f, 0.f, 0.f, 0.f);
             continue;
         }
@@ -308,11 +335,11 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
         const float kcf = (float)k_c;
 
         // ---- pixel offsets from the tile centre, in radians ----
-        float dx[PPT], dy[PPT], dz[PPT], nd2[PPT], ar[PPT], ai[PPT];
+        float dx[PPT], dy[PPT], dz[PPT], nd2[PPT], s0[PPT], ar[PPT], ai[PPT];
 #pragma unroll
         for (int k = 0; k < PPT; ++k) {
             const int ix = tx0 + lx, iy = ty0 + ly + k * ROWS;
-            dx[k] = dy[k] = dz[k] = nd2[k] = ar[k] = ai[k] = 0.0f;
+            dx[k] = dy[k] = dz[k] = nd2[k] = s0[k] = ar[k] = ai[k] = 0.0f;
             if (ix < nu && iy < nv) {
                 double x, y, z;
                 if (jb.r) {
@@ -334,6 +361,7 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
                     dy[k] = kcf * (float)(y - ti.rc[1]);
                     dz[k] = kcf * (float)(z - ti.rc[2]);
                     nd2[k] = -fmaf(dx[k], dx[k], fmaf(dy[k], dy[k], dz[k] * dz[k]));
+                    s0[k] = fmaf(ti.w0[2], dz[k], fmaf(ti.w0[1], dy[k], ti.w0[0] * dx[k]));
                 }
             }
         }
@@ -347,9 +375,14 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
                 const int b = c & 1;
                 bar_sync(kBarFull0 + b);
                 const int p0 = c * sh.C;
-                accumulate_any<PPT>(sm.s_mode[b], ti.planar != 0, min(sh.C, P - p0), sm.rec + b * cmax,
-                                    stage_base + (uint32_t)(b * stage_cap) * 16u, pstride, ilk, hi, dx, dy,
-                                    dz, nd2, ar, ai);
+                const uint32_t poff = stage_base + (uint32_t)(b * stage_cap) * 16u;
+                const int nc = min(sh.C, P - p0);
+                if (ti.wide)
+                    accumulate_mode<true, PPT>(sm.s_mode[b], ti.planar != 0, nc, sm.rec + b * cmax, poff,
+                                               pstride, ilk, hi, dx, dy, dz, nd2, s0, ar, ai);
+                else
+                    accumulate_mode<false, PPT>(sm.s_mode[b], ti.planar != 0, nc, sm.rec + b * cmax, poff,
+                                                pstride, ilk, hi, dx, dy, dz, nd2, s0, ar, ai);
                 bar_arrive(kBarEmpty0 + b);
             }
         }

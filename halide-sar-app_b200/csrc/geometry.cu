@@ -2,10 +2,13 @@
 //
 // tile_setup_kernel (one CTA per (job, tile)):
 //   rc    = centre of the bounding box of the tile's pixel positions
+//   wide  = k_c * (bounding-box half-diagonal) > kWideRad; then w0 = unit
+//           vector from rc to the mid-aperture antenna
 //   rho   = max |(f32)(r - rc)|, the same f32 offsets the backprojection
 //           kernel forms, padded; K = ceil(1.004 rho / lsr) + 2
 //   fin   = exp(+j k_c dr(pixel, P/2)) per pixel (backprojection.cpp:135),
-//           dr = |pos| - |r - pos| in f64, phase reduced in f64
+//           dr = |pos| - |r - pos| in f64, phase reduced in f64; wide tiles
+//           multiply in exp(-j w0 . k_c (r - rc)), also in f64
 // pulse_record_kernel (one thread per (tile, pulse)):
 //   w = pos - rc, R = |w|, dr_c = |pos| - R, t_c = (dr_c - lsa) / lsr,
 //   base = floor(t_c) - K, theta = k_c dr_c reduced to [-pi, pi),
@@ -84,13 +87,28 @@ __global__ void __launch_bounds__(kThreadsGeom) tile_setup_kernel(const DevJob *
         mn[1] = fmin(mn[1], y); mx[1] = fmax(mx[1], y);
         mn[2] = fmin(mn[2], z); mx[2] = fmax(mx[2], z);
     }
-    double rc[3];
+    double rc[3], hd2 = 0.0;
     for (int d = 0; d < 3; ++d) {
         const double a = block_reduce(mn[d], sd, MinOp()), b = block_reduce(mx[d], sd, MaxOp());
         rc[d] = a <= b ? 0.5 * (a + b) : 0.0;
+        if (a <= b) hd2 += 0.25 * (b - a) * (b - a);
     }
     const double k_c = jb.sc->k_c;
     const double4 pm = jb.pulse[jb.P / 2];
+    // wide tile: reference direction w0 toward the mid-aperture antenna; the
+    // phase w0 . k_c (r - rc) leaves the pulse loop and enters fin in f64
+    float w0f[3] = {0.f, 0.f, 0.f};
+    bool wide = false;
+    {
+        const double gx = pm.x - rc[0], gy = pm.y - rc[1], gz = pm.z - rc[2];
+        const double g = sqrt(gx * gx + gy * gy + gz * gz);
+        if (k_c * sqrt(hd2) > kWideRad && g > 0.0 && isfinite(g)) {
+            wide = true;
+            w0f[0] = (float)(gx / g);
+            w0f[1] = (float)(gy / g);
+            w0f[2] = (float)(gz / g);
+        }
+    }
     float rho = 0.0f;
     int planar = 1;
     for (int idx = threadIdx.x; idx < TX * TY; idx += blockDim.x) {
@@ -106,6 +124,11 @@ __global__ void __launch_bounds__(kThreadsGeom) tile_setup_kernel(const DevJob *
             const double ex = x - pm.x, ey = y - pm.y, ez = z - pm.z;
             const double drm = pm.w - sqrt(ex * ex + ey * ey + ez * ez);
             double th = drm * (k_c * kInv2Pi);
+            if (wide) {
+                const double s0 = k_c * ((double)w0f[0] * (x - rc[0]) + (double)w0f[1] * (y - rc[1]) +
+                                         (double)w0f[2] * (z - rc[2]));
+                th -= s0 * kInv2Pi;
+            }
             th = th - rint(th);
             float s, c;
             sincospif(2.0f * (float)th, &s, &c);
@@ -124,6 +147,10 @@ __global__ void __launch_bounds__(kThreadsGeom) tile_setup_kernel(const DevJob *
         t.rho = rho * (1.0f + 1e-5f) + 1e-6f;
         t.K = (int)ceilf(t.rho * (float)jb.inv_lsr * 1.004f) + 2;
         t.planar = planar;
+        t.wide = wide ? 1 : 0;
+        t.w0[0] = w0f[0];
+        t.w0[1] = w0f[1];
+        t.w0[2] = w0f[2];
         t.pad = 0;
         jb.tiles[wi.tile] = t;
         if (bad) atomicOr(&jb.sc->status, kStatusNonFinite);
@@ -154,17 +181,24 @@ __global__ void __launch_bounds__(kThreadsGeom) pulse_record_kernel(const DevJob
         const double theta = kTwoPi * th;  // in [-pi, pi]
         const float gm = (float)(t.rho * 0.5 * iR);                    // max |g| = rho / (2R)
         const float kcf = (float)k_c;
-        const float e2 = 2.0f * t.rho * gm * gm * kcf;                 // 2-term truncation (rad)
-        const float e3 = 5.0f * t.rho * gm * gm * gm * kcf;            // 3-term truncation (rad)
-        const int order = (e3 > kPhaseTol || gm > 1e-3f) ? 2 : (e2 > kPhaseTol ? 1 : 0);
+        // truncation of the series after 2, 3, 4 terms: C_n y^n |h| with
+        // y <= gm and |h| <= k_c rho (rad)
+        const float rk = t.rho * kcf;
+        const float e2 = 2.0f * rk * gm * gm;
+        const float e3 = 5.0f * rk * gm * gm * gm;
+        const float e4 = 14.0f * rk * gm * gm * gm * gm;
+        const int order = (e4 > kPhaseTol || gm > 5e-3f) ? 3 : e3 > kPhaseTol ? 2 : e2 > kPhaseTol ? 1 : 0;
         const int base = (int)fl - t.K;
-        rec.a = make_float4((float)(wx * iR), (float)(wy * iR), (float)(wz * iR), (float)(0.5 * iR / k_c));
+        const double ox = t.wide ? (double)t.w0[0] : 0.0, oy = t.wide ? (double)t.w0[1] : 0.0,
+                     oz = t.wide ? (double)t.w0[2] : 0.0;
+        rec.a = make_float4((float)(wx * iR - ox), (float)(wy * iR - oy), (float)(wz * iR - oz),
+                            (float)(0.5 * iR / k_c));
         const double c0 = (tc - fl) + ((double)t.K - 0.5) - theta * (jb.inv_lsr / k_c);
-        rec.b = make_float4((float)c0, (float)theta, (float)(k_c * R), __int_as_float(4 * base + order));
+        rec.b = make_float4((float)c0, (float)theta, (float)(k_c * R), __int_as_float(8 * base + order));
     } else {
         // no contribution: the staging leaves this pulse's window at zero
         rec.a = make_float4(0.f, 0.f, 0.f, 0.f);
-        rec.b = make_float4((float)t.K - 0.5f, 0.f, 1.f, __int_as_float(3));
+        rec.b = make_float4((float)t.K - 0.5f, 0.f, 1.f, __int_as_float(kOrderInvalid));
         atomicOr(&jb.sc->status, kStatusNonFinite);
     }
     jb.recs[(size_t)wi.tile * jb.P + p] = rec;

@@ -30,18 +30,29 @@ struct JobScalars {
     int pad[3];
 };
 
+// Tiles wider than this many radians of k_c * (half-diagonal) are "wide":
+// FP32 rounding of w_hat . d (about |d| * 2^-24) would exceed the phase
+// budget, so the linear phase toward a reference direction w0 is taken out
+// of the pulse loop and applied in f64 through the final phase.
+constexpr double kWideRad = 1024.0;
+constexpr int kOrderInvalid = 7;
+
 // Geometry of one pixel tile (tile-set-up kernel -> backprojection).
 struct __align__(16) TileInfo {
     double rc[3];  // centre of the tile's bounding box
     float rho;     // max |r - rc| over the tile, padded (m)
     int K;         // range window half-width (bins): W = 2K + 1
     int planar;    // 1 when every pixel has r.z == rc.z
+    int wide;      // 1: records hold w_hat - w0, fin carries exp(-j w0 . d)
+    float w0[3];   // unit direction from rc to the mid-aperture antenna (wide tiles)
     int pad;
 };
 
 // Per-(tile, pulse) constants (pulse-record kernel -> backprojection):
-//   a = (w_hat.x, w_hat.y, w_hat.z, e = 1/(2 k_c R))
-//   b = (c0 - theta*inv_lsr/k_c, theta, k_c R, int bits: 4*base + series order)
+//   a = (w_hat.x, w_hat.y, w_hat.z, e = 1/(2 k_c R)); wide tiles: w_hat - w0
+//   b = (c0 - theta*inv_lsr/k_c, theta, k_c R, int bits: 8*base + series order)
+// series order 0..3 (see the backprojection kernel); kOrderInvalid marks a
+// pulse that contributes nothing (non-finite geometry).
 struct __align__(16) PulseRec {
     float4 a;
     float4 b;

@@ -217,8 +217,9 @@ Runner::~Runner() {
 }
 
 int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cudaStream_t st,
-                    void *q_out) {
+                    void *q_out, bool for_graph) {
     const bool rc_only = q_out != nullptr;
+    auto rec = [&](int i) { return for_graph ? cudaSuccess : dev_->record(i, st); };
     if (njobs < 1 || !jobs) return fail(SARBP_ERR_INVALID, "no jobs");
     BpLaunch L = default_launch(opts, dev_->num_sms);
     // a tile shape without a 3-CTA/SM build runs at 2 unless the caller asked
@@ -244,6 +245,8 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         lay[i] = layout_of(jobs[i], off, L.tile_x, L.tile_y, rc_only, prec[i] == SARBP_PREC_NAIVE);
         off = lay[i].end;
     }
+    if (for_graph && scratch_.cap < off)
+        return fail(SARBP_ERR_STATE, "graph capture needs a prior run of the same jobs");
     cudaError_t e = scratch_.ensure(off, st);
     if (e != cudaSuccess) return cuda_fail(e, "allocating scratch");
     char *sbase = static_cast<char *>(scratch_.ptr);
@@ -277,8 +280,10 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
     const size_t o_items = align_up(o_rows + nrows_total * sizeof(RowItem), 256);
     const size_t o_cnt = align_up(o_items + items.size() * sizeof(WorkItem), 256);
     const size_t meta_bytes = o_cnt + 256;
+    if (for_graph && (host_meta_.cap < meta_bytes || meta_.cap < meta_bytes))
+        return fail(SARBP_ERR_STATE, "graph capture needs a prior run of the same jobs");
     // the previous batch's descriptor copy must have left host_meta_
-    e = cudaEventSynchronize(meta_done_);
+    e = for_graph ? cudaSuccess : cudaEventSynchronize(meta_done_);
     if (e != cudaSuccess) return cuda_fail(e, "waiting for the previous batch");
     e = host_meta_.ensure(meta_bytes);
     if (e != cudaSuccess) return cuda_fail(e, "allocating pinned descriptors");
@@ -356,7 +361,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
 
     e = cudaMemcpyAsync(d, h, meta_bytes, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return cuda_fail(e, "copying descriptors");
-    e = cudaEventRecord(meta_done_, st);
+    e = for_graph ? cudaSuccess : cudaEventRecord(meta_done_, st);
     if (e != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
 
     const DevJob *d_jobs = reinterpret_cast<const DevJob *>(d + o_jobs);
@@ -367,14 +372,16 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
     // twiddle tables first (a one-time synchronous upload per N_fft)
     for (size_t g = 0; g < row_groups.size(); ++g) {
         float2 *tw = nullptr;
+        if (for_graph && !dev_->twiddles.count(row_groups[g].first))
+            return fail(SARBP_ERR_STATE, "graph capture needs a prior run of the same jobs");
         e = dev_->twiddle(row_groups[g].first, &tw);
         if (e != cudaSuccess) return cuda_fail(e, "twiddle table");
     }
     for (int k = 0; k < DeviceInfo::kEvents; ++k) dev_->ev_recorded[k] = false;
-    if ((e = dev_->record(0, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    if ((e = rec(0)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
     launch_prep(d_jobs, njobs, st);
     dev_->launches++;
-    if ((e = dev_->record(1, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    if ((e = rec(1)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
     for (size_t g = 0; g < row_groups.size(); ++g) {
         const int logN = row_groups[g].first;
         const size_t first = row_groups[g].second;
@@ -386,7 +393,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         if (e != cudaSuccess) return cuda_fail(e, "range compression launch");
         dev_->launches++;
     }
-    if ((e = dev_->record(2, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    if ((e = rec(2)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
     if (rc_only) {
         e = cudaMemcpyAsync(q_out, hj[0].Q, (size_t)jobs[0].npulses * jobs[0].n_fft * sizeof(float2),
                             cudaMemcpyDeviceToDevice, st);
@@ -404,7 +411,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         if (e != cudaSuccess) return cuda_fail(e, "tile geometry launch");
         dev_->launches += 2;
     }
-    if ((e = dev_->record(3, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    if ((e = rec(3)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
     if (!items.empty()) {
         if (L.persistent) {
             const int occ = bp_max_active_blocks(L);
@@ -420,7 +427,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         if (e != cudaSuccess) return cuda_fail(e, "naive backprojection launch");
         dev_->launches++;
     }
-    if ((e = dev_->record(4, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    if ((e = rec(4)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
     bool any_u8 = false;
     long long max_px = 0;
     for (int i = 0; i < njobs; ++i) {
@@ -431,7 +438,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         e = launch_batch_u8(d_jobs, njobs, max_px, st);
         if (e != cudaSuccess) return cuda_fail(e, "u8 launch");
         dev_->launches++;
-        if ((e = dev_->record(5, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+        if ((e = rec(5)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
     }
     last_njobs_ = njobs;
     last_status_dev_ = reinterpret_cast<int *>(sbase);

@@ -63,8 +63,14 @@ public:
     // (no device work is enqueued on a validation error).
     // With q_out set, only range compression runs and job 0's profiles are
     // copied there.
+    // With for_graph set the call is being captured into a CUDA graph: no
+    // stage events, no wait on the previous descriptor copy (the captured
+    // copy re-reads this Runner's pinned descriptors at every replay, so the
+    // Runner must not enqueue anything else afterwards), and every buffer
+    // must already be large enough (an uncaptured enqueue of the same jobs
+    // comes first).
     int enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cudaStream_t st,
-                void *q_out = nullptr);
+                void *q_out = nullptr, bool for_graph = false);
     // Waits for the last batch and reads the kernels' status words.
     int check_status(cudaStream_t st);
     // Device footprint of the library scratch a job needs (bytes).

@@ -239,6 +239,50 @@ class Context:
         else:
             check(lib().sarbp_batch_device(self._h, arr, len(jobs), ctypes.byref(o)))
 
+    def autotune(self, jobs, precision=None):
+        """Fastest launch shape for this batch (sarbp_autotune); returns
+        (tune dict for run_jobs / plan, best ms or -1 when cached)."""
+        arr = (Job * len(jobs))(*jobs)
+        o = _opts(precision)
+        ms = ctypes.c_float()
+        check(lib().sarbp_autotune(self._h, arr, len(jobs), ctypes.byref(o), ctypes.byref(ms)))
+        tune = dict(tile=(o.tile_x, o.tile_y), pulse_chunk=o.pulse_chunk, min_blocks=o.min_blocks)
+        return tune, ms.value
+
+    def plan(self, jobs, precision=None, **tune):
+        """The batch captured as a CUDA graph (sarbp_plan_create)."""
+        return Plan(self, jobs, precision, **tune)
+
+
+class Plan:
+    """A CUDA-graph batch: launch(stream) replays it, wait() synchronises and
+    checks status, kernels is the kernel count per replay."""
+
+    def __init__(self, ctx, jobs, precision=None, **tune):
+        self._jobs = (Job * len(jobs))(*jobs)
+        o = _opts(precision, **tune)
+        self._h = ctypes.c_void_p()
+        check(lib().sarbp_plan_create(ctx._h, self._jobs, len(jobs), ctypes.byref(o),
+                                      ctypes.byref(self._h)))
+        self.kernels = lib().sarbp_plan_kernel_count(self._h)
+
+    def launch(self, stream=None):
+        check(lib().sarbp_plan_launch(self._h, stream))
+
+    def wait(self):
+        check(lib().sarbp_plan_wait(self._h))
+
+    def close(self):
+        if self._h:
+            lib().sarbp_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
 
 def make_job(nsamples, npulses, n_fft, taylor_s_l, nu, nv, delta_r, phs, k_r, pos, output_img,
              r=0, u=0, v=0, u_hat=(0, 0, 0), v_hat=(0, 0, 0), k_r64=0, pos64=0, out_u8=0,

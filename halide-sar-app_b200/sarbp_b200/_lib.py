@@ -78,6 +78,14 @@ SIGNATURES = {
         ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
         ctypes.c_double, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp,
         ctypes.POINTER(Opts)]),
+    "sarbp_plan_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job), ctypes.c_int,
+                                         ctypes.POINTER(Opts), ctypes.POINTER(ctypes.c_void_p)]),
+    "sarbp_plan_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "sarbp_plan_wait": (ctypes.c_int, [ctypes.c_void_p]),
+    "sarbp_plan_kernel_count": (ctypes.c_int, [ctypes.c_void_p]),
+    "sarbp_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "sarbp_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job), ctypes.c_int,
+                                      ctypes.POINTER(Opts), ctypes.POINTER(ctypes.c_float)]),
     "sarbp_backprojection_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job),
                                                    ctypes.POINTER(Opts)]),
     "sarbp_batch_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job), ctypes.c_int,

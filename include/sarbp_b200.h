@@ -173,6 +173,39 @@ int sarbp_batch_device(sarbp_ctx *ctx, const sarbp_job *jobs, int njobs,
                        const sarbp_opts *opts);
 
 /*
+ * A batch captured as a CUDA graph (no counterpart in the reference, which
+ * forms one image per call).  sarbp_plan_create runs the batch once (this
+ * writes the jobs' outputs and sizes the plan's own scratch), then captures
+ * the same launch sequence into a graph on a stream of the plan.
+ * sarbp_plan_launch replays it on cuda_stream (NULL: the plan's stream);
+ * the job arrays may hold new data between replays but keep their device
+ * addresses and shapes, and one replay must finish before the next starts
+ * (replays share the plan's scratch).  sarbp_plan_wait synchronises the
+ * last replay's stream and returns its status (as sarbp_ctx_synchronize).
+ */
+typedef struct sarbp_plan sarbp_plan;
+int sarbp_plan_create(sarbp_ctx *ctx, const sarbp_job *jobs, int njobs,
+                      const sarbp_opts *opts, sarbp_plan **out);
+int sarbp_plan_launch(sarbp_plan *plan, void *cuda_stream);
+int sarbp_plan_wait(sarbp_plan *plan);
+/* kernel nodes in the plan's graph (launches per replay) */
+int sarbp_plan_kernel_count(const sarbp_plan *plan);
+int sarbp_plan_destroy(sarbp_plan *plan);
+
+/*
+ * Launch-shape autotuner: runs the batch with each candidate pixel tile
+ * (32x32, 32x16, 64x16, 16x32, 32x8 at 3 CTAs/SM; 32x32, 32x64, 64x32,
+ * 16x64 at 2) and pulse-chunk depth (32, 64, 128), times set-up through
+ * backprojection with CUDA events, re-times the three fastest, and writes
+ * the fastest tile_x, tile_y, min_blocks and pulse_chunk into *inout (other
+ * fields kept).  The result is cached in the context under the batch's
+ * shape signature (sizes and precision), so a later call with the same
+ * shapes returns at once (*best_ms = -1 then).  Writes the jobs' outputs.
+ */
+int sarbp_autotune(sarbp_ctx *ctx, const sarbp_job *jobs, int njobs,
+                   sarbp_opts *inout, float *best_ms);
+
+/*
  * Backprojection of one device-resident job that allocates nothing (no
  * counterpart in the reference).  For callers that cannot allocate device
  * memory when they need an image -- inside a stream capture, under a memory
