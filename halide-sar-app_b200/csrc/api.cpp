@@ -74,6 +74,18 @@ int run_host_job(sarbp_ctx *ctx, const float *phs, int S, int P, const float *k_
     double *d_v = r ? nullptr : reinterpret_cast<double *>(base + o); o += b_v;
     double *d_out = reinterpret_cast<double *>(base + o);
     cudaStream_t st = ctx->stream;
+    // Row slabs: the pixel positions go up and the image comes down slab by
+    // slab while other slabs compute (images of 2^18 pixels and more).
+    int tile_x = 0, tile_y = 0;
+    Runner::tile_shape(opts, &tile_x, &tile_y);
+    const int tiles_y = (nv + tile_y - 1) / tile_y;
+    int nslabs = 0, slab_rows = 0;
+    if (precision != SARBP_PREC_NAIVE && npix >= ((size_t)1 << 18) && tiles_y >= 16) {
+        nslabs = std::min(sarbp_ctx::kMaxSlabs, tiles_y / 8);
+        slab_rows = (tiles_y + nslabs - 1) / nslabs;
+        nslabs = (tiles_y + slab_rows - 1) / slab_rows;
+    }
+    cudaStream_t cin = nslabs ? ctx->copy_in : st;
     struct Copy { void *dst; const void *src; size_t n; };
     const Copy copies[] = {
         {d_phs, phs, (size_t)S * P * 2 * sizeof(float)},
@@ -81,14 +93,37 @@ int run_host_job(sarbp_ctx *ctx, const float *phs, int S, int P, const float *k_
         {d_k64, k_r64, (size_t)S * sizeof(double)},
         {d_p32, pos32, (size_t)P * 3 * sizeof(float)},
         {d_p64, pos64, (size_t)P * 3 * sizeof(double)},
-        {d_r, r, npix * 3 * sizeof(double)},
+        {d_r, nslabs ? nullptr : r, npix * 3 * sizeof(double)},
         {d_u, r ? nullptr : plane->u, (size_t)nu * sizeof(double)},
         {d_v, r ? nullptr : plane->v, (size_t)nv * sizeof(double)},
     };
     for (const Copy &c : copies) {
         if (!c.src) continue;
-        e = cudaMemcpyAsync(c.dst, c.src, c.n, cudaMemcpyHostToDevice, st);
+        e = cudaMemcpyAsync(c.dst, c.src, c.n, cudaMemcpyHostToDevice, cin);
         if (e != cudaSuccess) return cuda_fail(e, "copying inputs to the device");
+    }
+    SlabSpec spec;
+    if (nslabs) {
+        if ((e = cudaEventRecord(ctx->ev_in, cin)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(st, ctx->ev_in, 0)) != cudaSuccess)
+            return cuda_fail(e, "ordering input copies");
+        for (int g = 0; g < nslabs && r; ++g) {
+            const size_t y0 = (size_t)g * slab_rows * tile_y;
+            const size_t y1 = std::min((size_t)nv, (size_t)(g + 1) * slab_rows * tile_y);
+            for (int c = 0; c < 3 && y1 > y0; ++c) {
+                const size_t off = (size_t)c * npix + y0 * (size_t)nu;
+                e = cudaMemcpyAsync(d_r + off, r + off, (y1 - y0) * (size_t)nu * sizeof(double),
+                                    cudaMemcpyHostToDevice, cin);
+                if (e != cudaSuccess) return cuda_fail(e, "copying pixel positions to the device");
+            }
+            if ((e = cudaEventRecord(ctx->ev_ready[g], cin)) != cudaSuccess)
+                return cuda_fail(e, "cudaEventRecord");
+        }
+        spec.nslabs = nslabs;
+        spec.tile_rows = slab_rows;
+        spec.aux = ctx->aux;
+        spec.ready = r ? ctx->ev_ready : nullptr;
+        spec.done = ctx->ev_done;
     }
     sarbp_job j;
     std::memset(&j, 0, sizeof(j));
@@ -115,10 +150,32 @@ int run_host_job(sarbp_ctx *ctx, const float *phs, int S, int P, const float *k_
     }
     j.output_img = d_out;
     j.precision = precision;
-    rc = ctx->runner->enqueue(&j, 1, opts, st);
-    if (rc) return rc;
-    e = cudaMemcpyAsync(out, d_out, npix * 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
-    if (e != cudaSuccess) return cuda_fail(e, "copying the image to the host");
+    rc = ctx->runner->enqueue(&j, 1, opts, st, nullptr, false, nslabs ? &spec : nullptr);
+    if (rc) {
+        // the copies may still read the caller's buffers
+        cudaStreamSynchronize(cin);
+        return rc;
+    }
+    if (!nslabs) {
+        e = cudaMemcpyAsync(out, d_out, npix * 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) return cuda_fail(e, "copying the image to the host");
+        return ctx->runner->check_status(st);
+    }
+    // output rows are flipped (backprojection.cpp:130): pixel rows [y0, y1)
+    // are image rows [nv - y1, nv - y0)
+    for (int g = 0; g < nslabs; ++g) {
+        const size_t y0 = (size_t)g * slab_rows * tile_y;
+        const size_t y1 = std::min((size_t)nv, (size_t)(g + 1) * slab_rows * tile_y);
+        if ((e = cudaStreamWaitEvent(ctx->copy_out, ctx->ev_done[g], 0)) != cudaSuccess)
+            return cuda_fail(e, "cudaStreamWaitEvent");
+        const size_t off = ((size_t)nv - y1) * (size_t)nu * 2;
+        e = cudaMemcpyAsync(out + off, d_out + off, (y1 - y0) * (size_t)nu * 2 * sizeof(double),
+                            cudaMemcpyDeviceToHost, ctx->copy_out);
+        if (e != cudaSuccess) return cuda_fail(e, "copying the image to the host");
+    }
+    if ((e = cudaEventRecord(ctx->ev_out, ctx->copy_out)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(st, ctx->ev_out, 0)) != cudaSuccess)
+        return cuda_fail(e, "ordering output copies");
     return ctx->runner->check_status(st);
 }
 
@@ -163,6 +220,18 @@ int sarbp_ctx_create(int device, sarbp_ctx **out) {
         return cuda_fail(e, "cudaStreamCreate");
     }
     ctx->stream = ctx->own_stream;
+    for (cudaStream_t *sp : {&ctx->copy_in, &ctx->aux, &ctx->copy_out})
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(sp, cudaStreamNonBlocking);
+    for (cudaEvent_t *ev : {&ctx->ev_in, &ctx->ev_out})
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+    for (int g = 0; g < sarbp_ctx::kMaxSlabs && e == cudaSuccess; ++g) {
+        e = cudaEventCreateWithFlags(&ctx->ev_ready[g], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_done[g], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) {
+        sarbp_ctx_destroy(ctx);
+        return cuda_fail(e, "creating streams and events");
+    }
     *out = ctx;
     return SARBP_OK;
 }
@@ -176,6 +245,14 @@ int sarbp_ctx_destroy(sarbp_ctx *ctx) {
     ctx->out_aux.release();
     ctx->dev.release();
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    for (cudaStream_t sp : {ctx->copy_in, ctx->aux, ctx->copy_out})
+        if (sp) cudaStreamDestroy(sp);
+    for (cudaEvent_t ev : {ctx->ev_in, ctx->ev_out})
+        if (ev) cudaEventDestroy(ev);
+    for (int g = 0; g < sarbp_ctx::kMaxSlabs; ++g) {
+        if (ctx->ev_ready[g]) cudaEventDestroy(ctx->ev_ready[g]);
+        if (ctx->ev_done[g]) cudaEventDestroy(ctx->ev_done[g]);
+    }
     delete ctx;
     return SARBP_OK;
 }

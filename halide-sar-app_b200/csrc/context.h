@@ -18,6 +18,12 @@ struct sarbp_ctx {
     sarbp::DeviceBuffer io;  // device copies of host-API inputs and outputs
     sarbp::DeviceBuffer out_aux;
     std::map<std::string, sarbp_opts> tuned;  // autotuner results by job-set key
+    // host-buffer entry points: copies in, second compute stream, copies out,
+    // and the events that pipeline row slabs between them
+    static constexpr int kMaxSlabs = 8;
+    cudaStream_t copy_in = nullptr, aux = nullptr, copy_out = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    cudaEvent_t ev_ready[kMaxSlabs] = {}, ev_done[kMaxSlabs] = {};
 };
 
 namespace sarbp {

@@ -214,11 +214,28 @@ Runner::~Runner() {
     meta_.release();
     host_meta_.release();
     if (meta_done_) cudaEventDestroy(meta_done_);
+    if (front_done_) cudaEventDestroy(front_done_);
+}
+
+void Runner::tile_shape(const sarbp_opts *opts, int *tile_x, int *tile_y) {
+    const BpLaunch L = default_launch(opts, 148);
+    *tile_x = L.tile_x;
+    *tile_y = L.tile_y;
 }
 
 int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cudaStream_t st,
-                    void *q_out, bool for_graph) {
+                    void *q_out, bool for_graph, const SlabSpec *slabs) {
     const bool rc_only = q_out != nullptr;
+    if (slabs && slabs->nslabs > 0) {
+        if (njobs != 1 || rc_only || for_graph || slabs->tile_rows < 1 || !slabs->aux || !slabs->done)
+            return fail(SARBP_ERR_INVALID, "row slabs need one job, a second stream and done events");
+        if (!front_done_) {
+            cudaError_t e = cudaEventCreateWithFlags(&front_done_, cudaEventDisableTiming);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaEventCreate");
+        }
+    } else {
+        slabs = nullptr;
+    }
     auto rec = [&](int i) { return for_graph ? cudaSuccess : dev_->record(i, st); };
     if (njobs < 1 || !jobs) return fail(SARBP_ERR_INVALID, "no jobs");
     BpLaunch L = default_launch(opts, dev_->num_sms);
@@ -279,7 +296,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
     const size_t o_rows = align_up(o_jobs + (size_t)njobs * sizeof(DevJob), 256);
     const size_t o_items = align_up(o_rows + nrows_total * sizeof(RowItem), 256);
     const size_t o_cnt = align_up(o_items + items.size() * sizeof(WorkItem), 256);
-    const size_t meta_bytes = o_cnt + 256;
+    const size_t meta_bytes = o_cnt + 256 * (size_t)(slabs ? slabs->nslabs : 1);
     if (for_graph && (host_meta_.cap < meta_bytes || meta_.cap < meta_bytes))
         return fail(SARBP_ERR_STATE, "graph capture needs a prior run of the same jobs");
     // the previous batch's descriptor copy must have left host_meta_
@@ -402,6 +419,40 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         last_status_dev_ = reinterpret_cast<int *>(sbase);
         return SARBP_OK;
     }
+    const bool slabbed = slabs && !items.empty() && prec[0] != SARBP_PREC_NAIVE;
+    if (slabbed) {
+        // ---- row slabs: geometry + backprojection per slab, two streams ----
+        if ((e = cudaEventRecord(front_done_, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+        const int tiles_x = (jobs[0].nu + L.tile_x - 1) / L.tile_x;
+        if (bp_max_active_blocks(L) < 1) return fail(SARBP_ERR_CUDA, "backprojection kernel does not fit on an SM");
+        for (int g = 0; g < slabs->nslabs; ++g) {
+            const size_t first = std::min(items.size(), (size_t)g * slabs->tile_rows * tiles_x);
+            const size_t last = std::min(items.size(), (size_t)(g + 1) * slabs->tile_rows * tiles_x);
+            cudaStream_t sg = (g & 1) ? slabs->aux : st;
+            if ((g & 1) && (e = cudaStreamWaitEvent(sg, front_done_, 0)) != cudaSuccess)
+                return cuda_fail(e, "cudaStreamWaitEvent");
+            if (slabs->ready && (e = cudaStreamWaitEvent(sg, slabs->ready[g], 0)) != cudaSuccess)
+                return cuda_fail(e, "cudaStreamWaitEvent");
+            if (last > first) {
+                const int n = (int)(last - first);
+                e = launch_tile_setup(d_jobs, d_items + first, n, sg);
+                if (e == cudaSuccess) e = launch_pulse_records(d_jobs, d_items + first, n, jobs[0].npulses, sg);
+                // one CTA per tile: the block scheduler then starts the next
+                // slab's CTAs (other stream) as this slab's last tiles finish
+                BpLaunch Lg = L;
+                Lg.persistent = 0;
+                Lg.grid = n;
+                if (e == cudaSuccess) e = launch_backproject(Lg, d_jobs, d_items + first, n, d_cnt + 64 * g, sg);
+                if (e != cudaSuccess) return cuda_fail(e, "slab launch");
+                dev_->launches += 3;
+            }
+            if ((e = cudaEventRecord(slabs->done[g], sg)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+        }
+        for (int g = 1; g < slabs->nslabs; g += 2)
+            if ((e = cudaStreamWaitEvent(st, slabs->done[g], 0)) != cudaSuccess)
+                return cuda_fail(e, "cudaStreamWaitEvent");
+        items.clear();  // formed above
+    }
     if (!items.empty()) {
         int max_p = 0;
         for (int i = 0; i < njobs; ++i)
@@ -427,6 +478,9 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         if (e != cudaSuccess) return cuda_fail(e, "naive backprojection launch");
         dev_->launches++;
     }
+    if (slabs && !slabbed)  // the whole image is final here
+        for (int g = 0; g < slabs->nslabs; ++g)
+            if ((e = cudaEventRecord(slabs->done[g], st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
     if ((e = rec(4)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
     bool any_u8 = false;
     long long max_px = 0;

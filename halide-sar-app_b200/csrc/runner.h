@@ -55,6 +55,22 @@ struct DeviceInfo {
     void release();
 };
 
+// Row slabs of a single job, for overlapping its host<->device copies with
+// compute: slab g covers tile rows [g * tile_rows, (g + 1) * tile_rows).
+// After prep and range compression (on the main stream), slab g's tile
+// geometry and backprojection run on the main stream (g even) or `aux`
+// (g odd) once `ready[g]` has fired (when set), and `done[g]` is recorded
+// when its pixels are final; the main stream joins every slab at the end.
+// Consecutive slabs sit on different streams so that one slab's CTAs fill
+// the SMs while the previous slab's last tiles finish.
+struct SlabSpec {
+    int nslabs = 0;
+    int tile_rows = 0;
+    cudaStream_t aux = nullptr;
+    const cudaEvent_t *ready = nullptr;  // [nslabs] or NULL
+    const cudaEvent_t *done = nullptr;   // [nslabs]
+};
+
 class Runner {
 public:
     explicit Runner(DeviceInfo *dev) : dev_(dev) {}
@@ -70,7 +86,9 @@ public:
     // must already be large enough (an uncaptured enqueue of the same jobs
     // comes first).
     int enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cudaStream_t st,
-                void *q_out = nullptr, bool for_graph = false);
+                void *q_out = nullptr, bool for_graph = false, const SlabSpec *slabs = nullptr);
+    // tile size the next enqueue with these options uses
+    static void tile_shape(const sarbp_opts *opts, int *tile_x, int *tile_y);
     // Waits for the last batch and reads the kernels' status words.
     int check_status(cudaStream_t st);
     // Device footprint of the library scratch a job needs (bytes).
@@ -81,6 +99,7 @@ private:
     DeviceBuffer scratch_, meta_;
     PinnedBuffer host_meta_;
     cudaEvent_t meta_done_ = nullptr;  // host_meta_ may be rewritten after this
+    cudaEvent_t front_done_ = nullptr; // range compression done (slabbed runs)
     int last_njobs_ = 0;
     int *last_status_dev_ = nullptr;   // status words of the last batch
     std::vector<int> status_host_;
