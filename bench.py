@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--stage-cap", type=int, default=0)
     ap.add_argument("--min-blocks", type=int, default=0)
     ap.add_argument("--njobs", type=int, default=96, help="batch96: number of jobs")
+    ap.add_argument("--serve-rates", default="20,50,100,200,400", help="serve: arrival rates (req/s)")
+    ap.add_argument("--serve-requests", type=int, default=2000, help="serve: requests per rate")
     return ap.parse_args()
 
 
@@ -544,6 +546,93 @@ def run_batch(args, rank, world, local_rank):
         print(json.dumps(out), flush=True)
 
 
+def run_serve(args, rank, world, local_rank):
+    """serve: the serving loop under Poisson arrivals.  A pool of 96 uneven
+    jobs (the batch96 distribution) lives in pinned host memory; each request
+    picks one (seeded), is submitted at its arrival time and returns its
+    complex image to pinned host memory.  Latency is submission to
+    image-on-host on the server's clock; p50/p99 over --serve-requests
+    requests per rate.  PREC_PRECISE (f64 positions and k_r)."""
+    import torch
+    import sarbp_b200 as sb
+    from sarbp_b200 import synth
+    from sarbp_b200.batch import HostJob
+
+    torch.cuda.set_device(local_rank)
+    pin = lambda shape, dtype: torch.empty(shape, dtype=getattr(torch, np.dtype(dtype).name)).pin_memory().numpy()
+    cfgs = synth.batch_jobs(njobs=96, seed=7 + rank)
+    t0 = time.time()
+    pool = [HostJob(c, alloc=pin) for c in cfgs]
+    outs = [hj.new_outputs()[0] for hj in pool]  # one image buffer per pool job (same image each time)
+    synth_s = time.time() - t0
+    ctx = sb.Context(local_rank)
+    rates = [float(x) for x in args.serve_rates.split(",")]
+    nreq = args.serve_requests
+    clocks = Clocks(gpu_uuid(torch, torch.device("cuda", local_rank))) if rank == 0 else None
+    sweep = []
+    srv = sb.Server(ctx, hbm_cap_bytes=150e9, lanes=2, max_batch=32, precision=sb.PREC_PRECISE)
+    try:
+        # warm-up: every pool job once
+        for k in range(len(pool)):
+            r = srv.submit(pool[k].job(outs[k], precision=sb.PREC_PRECISE))
+            srv.wait(r)
+            srv.release(r)
+        if clocks:
+            clocks.start()
+        for rate in rates:
+            rng = np.random.default_rng(int(rate * 1000) + rank)
+            pick = rng.integers(0, len(pool), nreq)
+            arrive = np.cumsum(rng.exponential(1.0 / rate, nreq))
+            b0 = srv.stats()["batches"]
+            rids = []
+            start = time.perf_counter()
+            for i in range(nreq):
+                while True:
+                    dt = arrive[i] - (time.perf_counter() - start)
+                    if dt <= 0:
+                        break
+                    time.sleep(dt if dt > 2e-3 else 0)
+                k = int(pick[i])
+                rids.append((srv.submit(pool[k].job(outs[k], precision=sb.PREC_PRECISE)), k))
+            lat, first, last, units = [], None, None, 0.0
+            for r, k in rids:
+                rc = srv.wait(r)
+                if rc != 0:
+                    raise RuntimeError("request failed: %d %s" % (rc, sb.last_error()))
+                ts, ta, td = srv.times(r)
+                lat.append((td - ts) * 1e3)
+                first = ts if first is None else min(first, ts)
+                last = td if last is None else max(last, td)
+                units += pool[k].units
+                srv.release(r)
+            lat = np.array(lat)
+            sweep.append({"rate_req_s": rate, "requests": nreq,
+                          "achieved_rate_req_s": nreq / (arrive[-1] if arrive[-1] > 0 else 1.0),
+                          "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                          "mean_ms": float(lat.mean()),
+                          "throughput_gpix_pulses_s": units / (last - first) / 1e9,
+                          "batches": srv.stats()["batches"] - b0})
+        clk = clocks.stop() if clocks else {}
+        peak = srv.stats()["peak_bytes"]
+    finally:
+        srv.close()
+        ctx.close()
+    top = sweep[-1]
+    out = {
+        "metric": "serving p99 latency at %g req/s (ms)" % top["rate_req_s"],
+        "value": top["p99_ms"], "unit": "ms", "n_gpus": world, "steps": nreq, "warmup": len(pool),
+        "ms_per_step": top["mean_ms"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (split-precision; f64 per-pulse set-up, PREC_PRECISE)",
+        "data": "synthetic (seeded uneven jobs, Poisson arrivals)",
+        "config": {"workload": "serve: %d requests per rate drawn from 96 uneven jobs (batch96 distribution), "
+                               "rates %s req/s, 2 lanes, batches <= 32, HBM budget 150 GB" % (nreq, args.serve_rates),
+                   "parallelism": "replicas%d" % world, "latency": "submission to complex image in pinned host memory"},
+        "sweep": sweep, "peak_device_bytes": peak, "clocks": clk, "synthesis_seconds": synth_s,
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -569,6 +658,8 @@ def main():
         with torch.cuda.stream(stream):
             if args.config == "batch96":
                 run_batch(args, rank, world, local_rank)
+            elif args.config == "serve":
+                run_serve(args, rank, world, local_rank)
             else:
                 run_ours(args, rank, world, local_rank)
     finally:

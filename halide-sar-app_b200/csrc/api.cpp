@@ -272,7 +272,7 @@ int sarbp_ctx_synchronize(sarbp_ctx *ctx) {
     return ctx->runner->check_status(ctx->stream);
 }
 
-long long sarbp_ctx_launch_count(sarbp_ctx *ctx) { return ctx ? ctx->dev.launches : -1; }
+long long sarbp_ctx_launch_count(sarbp_ctx *ctx) { return ctx ? ctx->dev.launches.load() : -1; }
 
 int sarbp_ctx_set_timing(sarbp_ctx *ctx, int on) {
     int rc = set_device(ctx);

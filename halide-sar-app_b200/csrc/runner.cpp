@@ -143,7 +143,13 @@ void PinnedBuffer::release() {
     cap = 0;
 }
 
+bool DeviceInfo::has_twiddle(int logN) {
+    std::lock_guard<std::mutex> lk(mu);
+    return twiddles.count(logN) != 0;
+}
+
 cudaError_t DeviceInfo::twiddle(int logN, float2 **out) {
+    std::lock_guard<std::mutex> lk(mu);
     auto it = twiddles.find(logN);
     if (it != twiddles.end()) {
         *out = it->second;
@@ -204,8 +210,8 @@ BpLaunch default_launch(const sarbp_opts *opts, int num_sms) {
     return L;
 }
 
-size_t Runner::job_scratch_bytes(const sarbp_job &j) {
-    const BpLaunch L = default_launch(nullptr, 148);
+size_t Runner::job_scratch_bytes(const sarbp_job &j, const sarbp_opts *opts) {
+    const BpLaunch L = default_launch(opts, 148);
     return layout_of(j, 0, L.tile_x, L.tile_y, false, j.precision == SARBP_PREC_NAIVE).end;
 }
 
@@ -213,6 +219,7 @@ Runner::~Runner() {
     scratch_.release();
     meta_.release();
     host_meta_.release();
+    status_pin_.release();
     if (meta_done_) cudaEventDestroy(meta_done_);
     if (front_done_) cudaEventDestroy(front_done_);
 }
@@ -236,7 +243,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
     } else {
         slabs = nullptr;
     }
-    auto rec = [&](int i) { return for_graph ? cudaSuccess : dev_->record(i, st); };
+    auto rec = [&](int i) { return (for_graph || !stage_events) ? cudaSuccess : dev_->record(i, st); };
     if (njobs < 1 || !jobs) return fail(SARBP_ERR_INVALID, "no jobs");
     BpLaunch L = default_launch(opts, dev_->num_sms);
     // a tile shape without a 3-CTA/SM build runs at 2 unless the caller asked
@@ -262,11 +269,42 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         lay[i] = layout_of(jobs[i], off, L.tile_x, L.tile_y, rc_only, prec[i] == SARBP_PREC_NAIVE);
         off = lay[i].end;
     }
-    if (for_graph && scratch_.cap < off)
+    if (for_graph && (scratch_.cap < off || pool_ || status_pin_.cap < njobs * sizeof(JobScalars)))
         return fail(SARBP_ERR_STATE, "graph capture needs a prior run of the same jobs");
-    cudaError_t e = scratch_.ensure(off, st);
-    if (e != cudaSuccess) return cuda_fail(e, "allocating scratch");
-    char *sbase = static_cast<char *>(scratch_.ptr);
+    cudaError_t e;
+    char *sbase = nullptr;
+    // pool mode: this batch's scratch comes from the pool and goes back to it
+    // stream-ordered behind the batch (on every exit path)
+    struct PoolBlock {
+        void *p = nullptr;
+        cudaStream_t st = nullptr;
+        ~PoolBlock() {
+            if (p) cudaFreeAsync(p, st);
+        }
+    } pooled;
+    if (pool_) {
+        pooled.st = st;
+        e = cudaMallocFromPoolAsync(&pooled.p, off, pool_, st);
+        if (e != cudaSuccess) {
+            pooled.p = nullptr;
+            return cuda_fail(e, "allocating scratch");
+        }
+        sbase = static_cast<char *>(pooled.p);
+    } else {
+        e = scratch_.ensure(off, st);
+        if (e != cudaSuccess) return cuda_fail(e, "allocating scratch");
+        sbase = static_cast<char *>(scratch_.ptr);
+    }
+    // status words come back through a pinned copy enqueued behind the batch
+    if (status_pin_.cap < njobs * sizeof(JobScalars)) {
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "synchronising the stream");
+        if ((e = status_pin_.ensure(njobs * sizeof(JobScalars))) != cudaSuccess)
+            return cuda_fail(e, "allocating pinned status words");
+    }
+    auto copy_status = [&]() -> cudaError_t {
+        last_njobs_ = njobs;
+        return cudaMemcpyAsync(status_pin_.ptr, sbase, njobs * sizeof(JobScalars), cudaMemcpyDeviceToHost, st);
+    };
 
     // ---- rows grouped by N_fft, work items longest first ----
     std::map<int, std::vector<RowItem>> rows;
@@ -389,12 +427,13 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
     // twiddle tables first (a one-time synchronous upload per N_fft)
     for (size_t g = 0; g < row_groups.size(); ++g) {
         float2 *tw = nullptr;
-        if (for_graph && !dev_->twiddles.count(row_groups[g].first))
+        if (for_graph && !dev_->has_twiddle(row_groups[g].first))
             return fail(SARBP_ERR_STATE, "graph capture needs a prior run of the same jobs");
         e = dev_->twiddle(row_groups[g].first, &tw);
         if (e != cudaSuccess) return cuda_fail(e, "twiddle table");
     }
-    for (int k = 0; k < DeviceInfo::kEvents; ++k) dev_->ev_recorded[k] = false;
+    if (stage_events)
+        for (int k = 0; k < DeviceInfo::kEvents; ++k) dev_->ev_recorded[k] = false;
     if ((e = rec(0)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
     launch_prep(d_jobs, njobs, st);
     dev_->launches++;
@@ -415,8 +454,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         e = cudaMemcpyAsync(q_out, hj[0].Q, (size_t)jobs[0].npulses * jobs[0].n_fft * sizeof(float2),
                             cudaMemcpyDeviceToDevice, st);
         if (e != cudaSuccess) return cuda_fail(e, "copying range profiles");
-        last_njobs_ = njobs;
-        last_status_dev_ = reinterpret_cast<int *>(sbase);
+        if ((e = copy_status()) != cudaSuccess) return cuda_fail(e, "copying job status");
         return SARBP_OK;
     }
     const bool slabbed = slabs && !items.empty() && prec[0] != SARBP_PREC_NAIVE;
@@ -494,18 +532,15 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         dev_->launches++;
         if ((e = rec(5)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
     }
-    last_njobs_ = njobs;
-    last_status_dev_ = reinterpret_cast<int *>(sbase);
+    if ((e = copy_status()) != cudaSuccess) return cuda_fail(e, "copying job status");
     return SARBP_OK;
 }
 
 int Runner::check_status(cudaStream_t st) {
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_fail(e, "synchronising the stream");
-    if (!last_status_dev_ || last_njobs_ == 0) return SARBP_OK;
-    std::vector<JobScalars> sc(last_njobs_);
-    e = cudaMemcpy(sc.data(), last_status_dev_, sc.size() * sizeof(JobScalars), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return cuda_fail(e, "reading job status");
+    if (last_njobs_ == 0 || !status_pin_.ptr) return SARBP_OK;
+    const JobScalars *sc = static_cast<const JobScalars *>(status_pin_.ptr);
     for (int i = 0; i < last_njobs_; ++i) {
         const int s = sc[i].status;
         if (s & kStatusNonFinite)

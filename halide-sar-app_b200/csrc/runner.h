@@ -8,7 +8,9 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -19,6 +21,7 @@
 namespace sarbp {
 
 void set_error(const std::string &msg);
+const char *last_error_cstr();
 int fail(int code, const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);
 
@@ -41,8 +44,9 @@ struct PinnedBuffer {
 struct DeviceInfo {
     int device = 0;
     int num_sms = 148;
-    std::map<int, float2 *> twiddles;  // logN -> device table
-    long long launches = 0;
+    std::map<int, float2 *> twiddles;  // logN -> device table (guarded by mu)
+    std::mutex mu;
+    std::atomic<long long> launches{0};
     // stage timing: events [0] before set-up, [1] after set-up, [2] after
     // range compression, [3] after tile geometry, [4] after backprojection,
     // [5] after u8
@@ -52,6 +56,7 @@ struct DeviceInfo {
     bool ev_recorded[kEvents] = {};
     cudaError_t record(int i, cudaStream_t st);
     cudaError_t twiddle(int logN, float2 **out);
+    bool has_twiddle(int logN);
     void release();
 };
 
@@ -92,7 +97,17 @@ public:
     // Waits for the last batch and reads the kernels' status words.
     int check_status(cudaStream_t st);
     // Device footprint of the library scratch a job needs (bytes).
-    static size_t job_scratch_bytes(const sarbp_job &j);
+    static size_t job_scratch_bytes(const sarbp_job &j, const sarbp_opts *opts = nullptr);
+    // Frees the scratch (the Runner must be idle).
+    void release_scratch() { scratch_.release(); }
+    // Take each batch's scratch from `pool` (stream-ordered) instead of the
+    // grow-only buffer; not for graph capture.
+    void use_pool(cudaMemPool_t pool) { pool_ = pool; }
+    // Scratch currently held (grow-only).
+    size_t scratch_capacity() const { return scratch_.cap + meta_.cap; }
+    // false: never record the context's stage-timing events (runners driven
+    // from another thread, e.g. the serving loop's lanes)
+    bool stage_events = true;
 
 private:
     DeviceInfo *dev_;
@@ -101,9 +116,8 @@ private:
     cudaEvent_t meta_done_ = nullptr;  // host_meta_ may be rewritten after this
     cudaEvent_t front_done_ = nullptr; // range compression done (slabbed runs)
     int last_njobs_ = 0;
-    int *last_status_dev_ = nullptr;   // status words of the last batch
-    std::vector<int> status_host_;
-    std::vector<int> last_status_stride_;
+    PinnedBuffer status_pin_;          // JobScalars of the last batch, copied behind it
+    cudaMemPool_t pool_ = nullptr;
 };
 
 BpLaunch default_launch(const sarbp_opts *opts, int num_sms);

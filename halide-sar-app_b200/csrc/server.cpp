@@ -1,0 +1,442 @@
+// server.cpp -- the serving loop: continuous batching of image-formation
+// requests under an HBM budget (no counterpart in the reference, which forms
+// one image per process run).
+//
+// A request is a sarbp_job whose pointers are HOST memory.  submit() only
+// queues it.  A scheduler thread forms batches: whenever one of the lanes
+// (a stream with its own Runner) is free it takes queued requests in arrival
+// order while their device footprint fits the budget, uploads each one's
+// phase history, k_r, positions and image-plane axes once into memory from
+// the server's pool, enqueues the batch (one persistent backprojection over
+// all the batch's tiles) and the copies of the images back to the host, and
+// frees the request memory stream-ordered behind them.  Requests that arrive
+// while other batches are on the GPU go into the next free lane, so batches
+// of different lanes overlap on the device.  A completion thread waits for
+// the lanes' batches in launch order, stamps the requests done and returns
+// their budget.
+//
+// Footprint of a request: its device inputs and outputs plus its share of
+// its batch's scratch, all taken from the server's memory pool when the
+// batch launches and returned stream-ordered behind it; the budget is
+// charged from admission to completion.  A request larger than the whole
+// budget fails with SARBP_ERR_ADMISSION.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "context.h"
+#include "runner.h"
+#include "sarbp_b200.h"
+
+using namespace sarbp;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+size_t a256(size_t x) { return (x + 255) / 256 * 256; }
+
+struct Request {
+    long long id = 0;
+    sarbp_job host{};  // the caller's job, host pointers
+    size_t io_bytes = 0, scratch_bytes = 0;
+    double work = 0.0;  // pixel*pulses
+    double t_submit = 0.0, t_start = 0.0, t_done = 0.0;
+    bool done = false;
+    int status = SARBP_OK;
+    std::string error;
+    void *dmem = nullptr;
+};
+
+// Device layout of a request's inputs and outputs (one pool allocation).
+struct IoLayout {
+    size_t phs, k32, k64, p32, p64, r, u, v, out, u8, end;
+};
+
+IoLayout io_layout(const sarbp_job &j) {
+    const size_t P = (size_t)j.npulses, S = (size_t)j.nsamples, npix = (size_t)j.nu * j.nv;
+    IoLayout L{};
+    size_t o = 0;
+    L.phs = o; o += a256(P * S * 8);
+    L.k32 = o; o += j.k_r ? a256(S * 4) : 0;
+    L.k64 = o; o += j.k_r64 ? a256(S * 8) : 0;
+    L.p32 = o; o += j.pos ? a256(P * 12) : 0;
+    L.p64 = o; o += j.pos64 ? a256(P * 24) : 0;
+    L.r = o; o += j.r ? a256(npix * 24) : 0;
+    L.u = o; o += (!j.r && j.u) ? a256((size_t)j.nu * 8) : 0;
+    L.v = o; o += (!j.r && j.v) ? a256((size_t)j.nv * 8) : 0;
+    L.out = o; o += a256(npix * 16);
+    L.u8 = o; o += j.out_u8 ? a256(npix) : 0;
+    L.end = o;
+    return L;
+}
+
+}  // namespace
+
+struct sarbp_server {
+    struct Lane {
+        cudaStream_t st = nullptr;
+        std::unique_ptr<Runner> runner;
+        cudaEvent_t done = nullptr;
+        std::vector<Request *> batch;
+        bool busy = false;
+        size_t charged = 0;  // budget charged for the batch in flight
+    };
+
+    sarbp_ctx *ctx = nullptr;
+    sarbp_opts launch{};
+    size_t cap = 0;
+    int max_batch = 32;
+    double max_work = 4e10;  // pixel*pulses per batch (bounds a batch's latency)
+    cudaMemPool_t pool = nullptr;
+    Clock::time_point t0 = Clock::now();
+
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<Request *> queue;
+    std::map<long long, std::unique_ptr<Request>> reqs;
+    long long next_id = 1;
+    size_t in_use = 0, peak = 0;
+    long long submitted = 0, completed = 0, batches = 0;
+    std::vector<Lane> lanes;
+    std::deque<Lane *> inflight;
+    bool stop = false, sched_exited = false;
+    std::thread sched, comp;
+
+    double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+
+    void scheduler();
+    void completer();
+    void launch_batch(Lane &L);
+};
+
+void sarbp_server::launch_batch(Lane &L) {
+    cudaSetDevice(ctx->dev.device);
+    std::vector<sarbp_job> jobs;
+    jobs.reserve(L.batch.size());
+    int rc = SARBP_OK;
+    std::string err;
+    for (Request *q : L.batch) {
+        const sarbp_job &h = q->host;
+        const IoLayout lay = io_layout(h);
+        cudaError_t e = cudaMallocFromPoolAsync(&q->dmem, lay.end, pool, L.st);
+        if (e != cudaSuccess) {
+            rc = cuda_fail(e, "serving: device memory for a request");
+            err = last_error_cstr();
+            q->dmem = nullptr;
+            break;
+        }
+        char *b = static_cast<char *>(q->dmem);
+        const size_t P = (size_t)h.npulses, S = (size_t)h.nsamples, npix = (size_t)h.nu * h.nv;
+        struct Copy { size_t off; const void *src; size_t n; };
+        const Copy in[] = {{lay.phs, h.phs, P * S * 8},     {lay.k32, h.k_r, S * 4},
+                           {lay.k64, h.k_r64, S * 8},       {lay.p32, h.pos, P * 12},
+                           {lay.p64, h.pos64, P * 24},      {lay.r, h.r, npix * 24},
+                           {lay.u, h.r ? nullptr : h.u, (size_t)h.nu * 8},
+                           {lay.v, h.r ? nullptr : h.v, (size_t)h.nv * 8}};
+        for (const Copy &c : in)
+            if (c.src && e == cudaSuccess) e = cudaMemcpyAsync(b + c.off, c.src, c.n, cudaMemcpyHostToDevice, L.st);
+        if (e != cudaSuccess) {
+            rc = cuda_fail(e, "serving: uploading a request");
+            err = last_error_cstr();
+            break;
+        }
+        sarbp_job d = h;
+        d.phs = reinterpret_cast<const float *>(b + lay.phs);
+        d.k_r = h.k_r ? reinterpret_cast<const float *>(b + lay.k32) : nullptr;
+        d.k_r64 = h.k_r64 ? reinterpret_cast<const double *>(b + lay.k64) : nullptr;
+        d.pos = h.pos ? reinterpret_cast<const float *>(b + lay.p32) : nullptr;
+        d.pos64 = h.pos64 ? reinterpret_cast<const double *>(b + lay.p64) : nullptr;
+        d.r = h.r ? reinterpret_cast<const double *>(b + lay.r) : nullptr;
+        d.u = (!h.r && h.u) ? reinterpret_cast<const double *>(b + lay.u) : nullptr;
+        d.v = (!h.r && h.v) ? reinterpret_cast<const double *>(b + lay.v) : nullptr;
+        d.output_img = reinterpret_cast<double *>(b + lay.out);
+        d.out_u8 = h.out_u8 ? reinterpret_cast<uint8_t *>(b + lay.u8) : nullptr;
+        jobs.push_back(d);
+    }
+    if (rc == SARBP_OK) {
+        rc = L.runner->enqueue(jobs.data(), (int)jobs.size(), &launch, L.st);
+        if (rc) err = last_error_cstr();
+    }
+    if (rc == SARBP_OK) {
+        for (size_t i = 0; i < jobs.size() && rc == SARBP_OK; ++i) {
+            const sarbp_job &h = L.batch[i]->host;
+            const size_t npix = (size_t)h.nu * h.nv;
+            cudaError_t e = cudaSuccess;
+            if (h.output_img)
+                e = cudaMemcpyAsync(h.output_img, jobs[i].output_img, npix * 16, cudaMemcpyDeviceToHost, L.st);
+            if (e == cudaSuccess && h.out_u8)
+                e = cudaMemcpyAsync(h.out_u8, jobs[i].out_u8, npix, cudaMemcpyDeviceToHost, L.st);
+            if (e != cudaSuccess) {
+                rc = cuda_fail(e, "serving: copying an image to the host");
+                err = last_error_cstr();
+            }
+        }
+    }
+    for (Request *q : L.batch) {
+        if (q->dmem) cudaFreeAsync(q->dmem, L.st);
+        q->dmem = nullptr;
+        if (rc) {
+            q->status = rc;
+            q->error = err;
+        }
+    }
+    cudaEventRecord(L.done, L.st);
+}
+
+void sarbp_server::scheduler() {
+    cudaSetDevice(ctx->dev.device);
+    std::unique_lock<std::mutex> lk(mu);
+    auto free_lane = [&]() -> Lane * {
+        for (Lane &L : lanes)
+            if (!L.busy) return &L;
+        return nullptr;
+    };
+    for (;;) {
+        cv.wait(lk, [&] { return (stop && queue.empty()) || (!queue.empty() && free_lane()); });
+        if (queue.empty()) {
+            sched_exited = true;
+            cv.notify_all();
+            return;
+        }
+        Lane &L = *free_lane();
+        // admission: arrival order, while the batch fits the budget
+        std::vector<Request *> batch;
+        size_t bytes = 0;
+        double work = 0.0;
+        while (!queue.empty() && (int)batch.size() < max_batch) {
+            Request *q = queue.front();
+            const size_t need = q->io_bytes + q->scratch_bytes;
+            if (!batch.empty() && work + q->work > max_work) break;
+            if (in_use + bytes + need > cap) {
+                if (need > cap) {  // cannot fit even an idle server
+                    queue.pop_front();
+                    q->status = SARBP_ERR_ADMISSION;
+                    q->error = "request needs " + std::to_string(need >> 20) +
+                               " MiB of device memory, more than the server budget of " +
+                               std::to_string(cap >> 20) + " MiB";
+                    q->done = true;
+                    q->t_done = now();
+                    ++completed;
+                    cv.notify_all();
+                    continue;
+                }
+                break;  // wait for memory to free up
+            }
+            queue.pop_front();
+            batch.push_back(q);
+            bytes += need;
+            work += q->work;
+        }
+        if (batch.empty()) {
+            // the head request waits for memory: sleep until a batch completes
+            if (!inflight.empty()) {
+                const long long before = completed;
+                cv.wait(lk, [&] { return stop || completed != before; });
+            }
+            continue;
+        }
+        in_use += bytes;
+        L.charged = bytes;
+        peak = std::max(peak, in_use);
+        const double t = now();
+        for (Request *q : batch) q->t_start = t;
+        L.batch = std::move(batch);
+        L.busy = true;
+        ++batches;
+        lk.unlock();
+        launch_batch(L);
+        lk.lock();
+        inflight.push_back(&L);
+        cv.notify_all();
+    }
+}
+
+void sarbp_server::completer() {
+    cudaSetDevice(ctx->dev.device);
+    std::unique_lock<std::mutex> lk(mu);
+    for (;;) {
+        cv.wait(lk, [&] { return !inflight.empty() || sched_exited; });
+        if (inflight.empty()) return;
+        Lane &L = *inflight.front();
+        lk.unlock();
+        cudaError_t e = cudaEventSynchronize(L.done);
+        int rc = e == cudaSuccess ? L.runner->check_status(L.st) : cuda_fail(e, "serving: waiting for a batch");
+        std::string err = rc ? last_error_cstr() : std::string();
+        const double t = now();
+        lk.lock();
+        for (Request *q : L.batch) {
+            if (q->status == SARBP_OK && rc) {
+                q->status = rc;
+                q->error = err;
+            }
+            q->t_done = t;
+            q->done = true;
+            ++completed;
+        }
+        in_use -= L.charged;
+        L.charged = 0;
+        L.batch.clear();
+        L.busy = false;
+        inflight.pop_front();
+        cv.notify_all();
+    }
+}
+
+extern "C" {
+
+int sarbp_server_create(sarbp_ctx *ctx, const sarbp_opts *launch, double hbm_cap_bytes, int lanes,
+                        int max_batch, sarbp_server **out) {
+    int rc = ctx_set_device(ctx);
+    if (rc) return rc;
+    if (!out) return fail(SARBP_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!(hbm_cap_bytes > 0)) return fail(SARBP_ERR_INVALID, "the HBM budget must be positive");
+    auto s = std::make_unique<sarbp_server>();
+    s->ctx = ctx;
+    if (launch) s->launch = *launch;
+    s->cap = (size_t)hbm_cap_bytes;
+    s->max_batch = max_batch > 0 ? max_batch : 32;
+    const int nl = lanes > 0 ? std::min(lanes, 8) : 2;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = ctx->dev.device;
+    cudaError_t e = cudaMemPoolCreate(&s->pool, &props);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemPoolCreate");
+    unsigned long long keep = (unsigned long long)s->cap;
+    cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    s->lanes.resize(nl);
+    for (auto &L : s->lanes) {
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming);
+        L.runner = std::make_unique<Runner>(&ctx->dev);
+        L.runner->stage_events = false;
+        L.runner->use_pool(s->pool);
+    }
+    if (e == cudaSuccess) {
+        // back the pool with memory up front so that first batches do not
+        // pay for physical allocation (kept: the release threshold is the cap)
+        const size_t warm = std::min<size_t>(s->cap, (size_t)8 << 30);
+        void *p = nullptr;
+        e = cudaMallocFromPoolAsync(&p, warm, s->pool, s->lanes[0].st);
+        if (e == cudaSuccess) e = cudaFreeAsync(p, s->lanes[0].st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->lanes[0].st);
+    }
+    if (e != cudaSuccess) {
+        for (auto &L : s->lanes) {
+            if (L.st) cudaStreamDestroy(L.st);
+            if (L.done) cudaEventDestroy(L.done);
+        }
+        cudaMemPoolDestroy(s->pool);
+        return cuda_fail(e, "creating serving lanes");
+    }
+    sarbp_server *p = s.release();
+    p->sched = std::thread([p] { p->scheduler(); });
+    p->comp = std::thread([p] { p->completer(); });
+    *out = p;
+    return SARBP_OK;
+}
+
+int sarbp_server_submit(sarbp_server *s, const sarbp_job *host_job, long long *id) {
+    if (!s || !host_job || !id) return fail(SARBP_ERR_INVALID, "bad submit arguments");
+    const sarbp_job &j = *host_job;
+    if (j.nsamples < 1 || j.npulses < 1 || j.nu < 1 || j.nv < 1 || !j.phs ||
+        !(j.k_r || j.k_r64) || !(j.pos || j.pos64) || !(j.r || (j.u && j.v)))
+        return fail(SARBP_ERR_INVALID, "request: sizes, phs, k_r, pos and pixel positions are required");
+    auto q = std::make_unique<Request>();
+    q->host = j;
+    q->io_bytes = io_layout(j).end;
+    q->scratch_bytes = Runner::job_scratch_bytes(j, &s->launch) + (64u << 10);
+    q->work = (double)j.nu * j.nv * j.npulses;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) return fail(SARBP_ERR_STATE, "server is shutting down");
+    q->id = s->next_id++;
+    q->t_submit = s->now();
+    *id = q->id;
+    s->queue.push_back(q.get());
+    s->reqs[q->id] = std::move(q);
+    ++s->submitted;
+    s->cv.notify_all();
+    return SARBP_OK;
+}
+
+int sarbp_server_wait(sarbp_server *s, long long id, double timeout_s) {
+    if (!s) return fail(SARBP_ERR_INVALID, "server is NULL");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return fail(SARBP_ERR_INVALID, "unknown request id");
+    Request *q = it->second.get();
+    const auto until = Clock::now() + std::chrono::duration<double>(timeout_s < 0 ? 1e9 : timeout_s);
+    if (!s->cv.wait_until(lk, until, [&] { return q->done; }))
+        return fail(SARBP_ERR_TIMEOUT, "request " + std::to_string(id) + " not finished yet");
+    if (q->status) set_error(q->error);
+    return q->status;
+}
+
+int sarbp_server_times(sarbp_server *s, long long id, double *submit_s, double *start_s, double *done_s) {
+    if (!s) return fail(SARBP_ERR_INVALID, "server is NULL");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return fail(SARBP_ERR_INVALID, "unknown request id");
+    const Request &q = *it->second;
+    if (submit_s) *submit_s = q.t_submit;
+    if (start_s) *start_s = q.t_start;
+    if (done_s) *done_s = q.done ? q.t_done : -1.0;
+    return SARBP_OK;
+}
+
+int sarbp_server_release(sarbp_server *s, long long id) {
+    if (!s) return fail(SARBP_ERR_INVALID, "server is NULL");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return fail(SARBP_ERR_INVALID, "unknown request id");
+    if (!it->second->done) return fail(SARBP_ERR_STATE, "request still in flight");
+    s->reqs.erase(it);
+    return SARBP_OK;
+}
+
+int sarbp_server_stats(sarbp_server *s, long long *submitted, long long *completed, long long *batches,
+                       double *in_use_bytes, double *peak_bytes) {
+    if (!s) return fail(SARBP_ERR_INVALID, "server is NULL");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (submitted) *submitted = s->submitted;
+    if (completed) *completed = s->completed;
+    if (batches) *batches = s->batches;
+    if (in_use_bytes) *in_use_bytes = (double)s->in_use;
+    if (peak_bytes) *peak_bytes = (double)s->peak;
+    return SARBP_OK;
+}
+
+int sarbp_server_destroy(sarbp_server *s) {
+    if (!s) return SARBP_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        s->cv.notify_all();
+    }
+    if (s->sched.joinable()) s->sched.join();  // drains the queue
+    if (s->comp.joinable()) s->comp.join();    // waits for the lanes
+    cudaSetDevice(s->ctx->dev.device);
+    for (auto &L : s->lanes) {
+        if (L.st) cudaStreamSynchronize(L.st);
+        L.runner.reset();
+        if (L.st) cudaStreamDestroy(L.st);
+        if (L.done) cudaEventDestroy(L.done);
+    }
+    if (s->pool) cudaMemPoolDestroy(s->pool);
+    delete s;
+    return SARBP_OK;
+}
+
+}  // extern "C"

@@ -33,6 +33,11 @@ def _ptr(a):
     return ctypes.c_void_p(a.ctypes.data) if a is not None else ctypes.c_void_p(0)
 
 
+def last_error():
+    """Message of the calling thread's last failed call."""
+    return lib().sarbp_last_error().decode()
+
+
 def version():
     return lib().sarbp_version().decode()
 
@@ -252,6 +257,58 @@ class Context:
     def plan(self, jobs, precision=None, **tune):
         """The batch captured as a CUDA graph (sarbp_plan_create)."""
         return Plan(self, jobs, precision, **tune)
+
+
+class Server:
+    """The serving loop (sarbp_server_*): submit(job) queues a Job whose
+    pointers are host memory and returns its id; wait(id) returns its status
+    (ERR_TIMEOUT while in flight); times(id) gives (submit, start, done)
+    seconds on the server's clock."""
+
+    def __init__(self, ctx, hbm_cap_bytes=150e9, lanes=2, max_batch=32, precision=None, **tune):
+        o = _opts(precision, **tune)
+        self._h = ctypes.c_void_p()
+        check(lib().sarbp_server_create(ctx._h, ctypes.byref(o), float(hbm_cap_bytes), int(lanes),
+                                        int(max_batch), ctypes.byref(self._h)))
+        self._keep = {}
+
+    def submit(self, job, keep=None):
+        rid = ctypes.c_longlong()
+        check(lib().sarbp_server_submit(self._h, ctypes.byref(job), ctypes.byref(rid)))
+        self._keep[rid.value] = (job, keep)
+        return rid.value
+
+    def wait(self, rid, timeout=-1.0):
+        return int(lib().sarbp_server_wait(self._h, int(rid), float(timeout)))
+
+    def times(self, rid):
+        a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        check(lib().sarbp_server_times(self._h, int(rid), ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    def release(self, rid):
+        check(lib().sarbp_server_release(self._h, int(rid)))
+        self._keep.pop(rid, None)
+
+    def stats(self):
+        s, c, b = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        u, p = ctypes.c_double(), ctypes.c_double()
+        check(lib().sarbp_server_stats(self._h, ctypes.byref(s), ctypes.byref(c), ctypes.byref(b),
+                                       ctypes.byref(u), ctypes.byref(p)))
+        return dict(submitted=s.value, completed=c.value, batches=b.value, in_use_bytes=u.value,
+                    peak_bytes=p.value)
+
+    def close(self):
+        if self._h:
+            lib().sarbp_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Plan:

@@ -84,6 +84,18 @@ SIGNATURES = {
     "sarbp_plan_wait": (ctypes.c_int, [ctypes.c_void_p]),
     "sarbp_plan_kernel_count": (ctypes.c_int, [ctypes.c_void_p]),
     "sarbp_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "sarbp_server_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Opts), ctypes.c_double,
+                                           ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "sarbp_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job),
+                                           ctypes.POINTER(ctypes.c_longlong)]),
+    "sarbp_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double]),
+    "sarbp_server_times": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_double),
+                                          ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "sarbp_server_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
+    "sarbp_server_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
+                                          ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
+                                          ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "sarbp_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "sarbp_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job), ctypes.c_int,
                                       ctypes.POINTER(Opts), ctypes.POINTER(ctypes.c_float)]),
     "sarbp_backprojection_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job),

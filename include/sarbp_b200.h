@@ -193,6 +193,42 @@ int sarbp_plan_kernel_count(const sarbp_plan *plan);
 int sarbp_plan_destroy(sarbp_plan *plan);
 
 /*
+ * Serving loop (no counterpart in the reference): continuous batching of
+ * image-formation requests under a device-memory budget.  A request is a
+ * sarbp_job whose pointers are HOST memory (output_img and out_u8, each
+ * optional, receive the complex128 and u8 images); the caller keeps them
+ * valid until the request is done.  A scheduler thread admits queued
+ * requests in arrival order while their device footprint (inputs, outputs,
+ * and their batch's scratch) fits hbm_cap_bytes, uploads each phase history
+ * once, and launches them as one batch on the first free of `lanes` streams
+ * (default 2), at most max_batch requests per batch (default 32); batches of
+ * different lanes overlap on the device.  A request that cannot fit an idle
+ * server fails with SARBP_ERR_ADMISSION.  `launch` (may be NULL) fixes the
+ * precision and launch shape of every batch, so a request's image does not
+ * depend on what it was batched with.
+ */
+typedef struct sarbp_server sarbp_server;
+int sarbp_server_create(sarbp_ctx *ctx, const sarbp_opts *launch,
+                        double hbm_cap_bytes, int lanes, int max_batch,
+                        sarbp_server **out);
+int sarbp_server_submit(sarbp_server *server, const sarbp_job *host_job,
+                        long long *id);
+/* Waits up to timeout_s (< 0: no limit) for request id; returns its status,
+ * or SARBP_ERR_TIMEOUT while it is still queued or running. */
+int sarbp_server_wait(sarbp_server *server, long long id, double timeout_s);
+/* Seconds since the server started: submission, admission (batch launch),
+ * completion (images on the host; -1 while in flight). */
+int sarbp_server_times(sarbp_server *server, long long id, double *submit_s,
+                       double *start_s, double *done_s);
+/* Forgets a finished request. */
+int sarbp_server_release(sarbp_server *server, long long id);
+int sarbp_server_stats(sarbp_server *server, long long *submitted,
+                       long long *completed, long long *batches,
+                       double *in_use_bytes, double *peak_bytes);
+/* Finishes every queued and running request, then frees the server. */
+int sarbp_server_destroy(sarbp_server *server);
+
+/*
  * Launch-shape autotuner: runs the batch with each candidate pixel tile
  * (32x32, 32x16, 64x16, 16x32, 32x8 at 3 CTAs/SM; 32x32, 32x64, 64x32,
  * 16x64 at 2) and pulse-chunk depth (32, 64, 128), times set-up through

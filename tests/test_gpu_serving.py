@@ -1,0 +1,122 @@
+"""The serving loop (continuous batching under an HBM budget).
+
+* A request's image is the same alone and in a mix (bit for bit): the
+  server fixes the launch shape, and each pixel tile is formed by one CTA
+  whatever else shares the batch.
+* Served images in PREC_PRECISE agree with the FP64 oracle to relative L2
+  <= 1e-3 (the serving target) on a 5 % sample of the requests, at
+  sampled pixels.
+* Admission by footprint: requests that cannot fit the budget of an idle
+  server fail with ERR_ADMISSION; the others are served with the budget
+  never exceeded; overlapping submissions are batched.
+"""
+import time
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def pool():
+    from sarbp_b200 import synth
+    from sarbp_b200.batch import HostJob
+    cfgs = synth.batch_jobs(njobs=6, seed=21, sizes=(128, 256), pulses=(100, 400), samples=(256, 512))
+    return [HostJob(c) for c in cfgs]
+
+
+def _submit(srv, hj, precision):
+    out, u8 = hj.new_outputs()
+    job = hj.job(out, u8, precision=precision)
+    rid = srv.submit(job, keep=(out, u8))
+    return rid, out
+
+
+def test_same_alone_and_in_mix(ctx, sb, pool):
+    srv = sb.Server(ctx, hbm_cap_bytes=8e9, lanes=2, max_batch=8, precision=sb.PREC_PRECISE)
+    try:
+        rid, alone = _submit(srv, pool[0], sb.PREC_PRECISE)
+        assert srv.wait(rid, 60.0) == 0
+        mix = []
+        for i in range(24):
+            hj = pool[(i * 5) % len(pool)]
+            mix.append((hj, *_submit(srv, hj, sb.PREC_PRECISE)))
+        for hj, r, out in mix:
+            assert srv.wait(r, 60.0) == 0
+        twins = [out for hj, r, out in mix if hj is pool[0]]
+        assert twins
+        for out in twins:
+            assert np.array_equal(out, alone)
+        st = srv.stats()
+        assert st["completed"] == 25 and st["batches"] >= 2
+        assert st["peak_bytes"] <= 8e9
+        for hj, r, out in mix:
+            s, a, d = srv.times(r)
+            assert 0 <= s <= a <= d
+    finally:
+        srv.close()
+
+
+def test_served_vs_fp64_sample(ctx, sb, oracle, pool):
+    srv = sb.Server(ctx, hbm_cap_bytes=8e9, lanes=2, max_batch=8, precision=sb.PREC_PRECISE)
+    try:
+        reqs = []
+        for i in range(40):
+            hj = pool[i % len(pool)]
+            reqs.append((hj, *_submit(srv, hj, sb.PREC_PRECISE)))
+        for _, r, _ in reqs:
+            assert srv.wait(r, 120.0) == 0
+    finally:
+        srv.close()
+    rng = np.random.default_rng(3)
+    sample = rng.choice(len(reqs), size=max(2, len(reqs) // 20), replace=False)
+    for k in sample:
+        hj, _, out = reqs[k]
+        d = hj.data
+        r = oracle.pixel_locs(d["u"], d["v"], d["u_hat"], d["v_hat"])
+        idx = rng.choice(hj.nu * hj.nv, 1500, replace=False)
+        ref = oracle.backprojection(d["phs"], d["k_r"], d["taylor"], d["N_fft"], d["delta_r"], d["pos"], r,
+                                    hj.nu, hj.nv, mode=oracle.MODE_FP64, out_idx=idx)
+        e = rel_l2(out.ravel()[idx], ref)
+        print("served request %d (%dx%d, %d pulses): rel-L2 vs FP64 %.2e" % (k, hj.nu, hj.nv, hj.P, e))
+        assert e < 1e-3
+
+
+def test_admission_by_footprint(ctx, sb, pool):
+    from sarbp_b200 import _lib, synth
+    from sarbp_b200.batch import HostJob
+    cap = 256e6
+    srv = sb.Server(ctx, hbm_cap_bytes=cap, lanes=2, max_batch=4, precision=sb.PREC_COMPAT)
+    try:
+        big = HostJob(synth.batch_jobs(njobs=1, seed=2, sizes=(2048,), pulses=(1500, 1600),
+                                       samples=(1024,))[0])
+        rid_big, _ = _submit(srv, big, sb.PREC_COMPAT)
+        rids = [_submit(srv, pool[i % len(pool)], sb.PREC_COMPAT)[0] for i in range(12)]
+        assert srv.wait(rid_big, 60.0) == _lib.ERR_ADMISSION
+        for r in rids:
+            assert srv.wait(r, 60.0) == 0
+        st = srv.stats()
+        assert 0 < st["peak_bytes"] <= cap
+        assert st["completed"] == 13
+    finally:
+        srv.close()
+
+
+def test_wait_times_out_while_queued(ctx, sb, pool):
+    from sarbp_b200 import _lib
+    srv = sb.Server(ctx, hbm_cap_bytes=8e9, lanes=1, max_batch=1)
+    try:
+        rids = [_submit(srv, pool[i % len(pool)], sb.PREC_COMPAT)[0] for i in range(6)]
+        last = rids[-1]
+        # the last of six one-request batches on one lane cannot be done at once
+        t0 = time.perf_counter()
+        rc = srv.wait(last, 0.0)
+        assert rc in (0, _lib.ERR_TIMEOUT)
+        assert time.perf_counter() - t0 < 1.0
+        for r in rids:
+            assert srv.wait(r, 60.0) == 0
+    finally:
+        srv.close()
