@@ -101,16 +101,20 @@ __device__ __forceinline__ void bulk_copy(void *dst, const void *src, uint32_t b
 // Inner loop over the nc pulses of a chunk for a consumer's PPT pixels.
 // With h = s - e|d|^2 and y = e h, the exact range difference is the series
 //     Delta = h (1 + y + 2y^2 + 5y^3 + 14y^4 + ...)   (Catalan numbers)
-// MODE 0: Delta = s + e t, t = s^2 - |d|^2 (two terms);
-// MODE 1: s + e t (1 + 2 e s) (three terms);
-// MODE 2: h + h y (1 + 2y + 5y^2) (four terms), all FMA-pipe arithmetic;
-// MODE 3: the closed form 2R'h / (R' + sqrt(R'(R' - 2h))) (near field).
-// Modes 2 and 3 form the nonlinear part N = Delta - s on its own (mode 3 as
-// (s Delta - |d|^2) / (R' + r), free of the cancellation in Delta - s), so
-// their approximate divisions only see a small quantity.
+// MODE 0: Delta = s + e t, t = s^2 - |d|^2 (two terms); MODE 1 adds the
+// third term 2e^2 s t; MODE 2 the fourth, e^2 (-|d|^2 (h + s) + h^3 (2 + 5y))
+// over the two-term form; MODE 3 uses the closed form 2R'h / (R' + r),
+// r = sqrt(R'(R' - 2h)) (near field), as its nonlinear part
+// N = (s Delta - |d|^2) / (R' + r), free of the cancellation in Delta - s.
+// Narrow tiles: the records carry kappa w_hat, e' and sigma0 = kappa theta +
+// e theta^2 (pulse-record kernel), so the phase theta + s + e t is
+//     sigma = kappa w_hat . d + sigma0,   D = sigma + e' (sigma^2 - |d|^2)
+// (three FMAs for a planar tile), plus from MODE 1 on the small terms
+// (e - e')(-|d|^2) and the higher series terms, formed from
+// s ~= sigma - sigma0 (relative error ~1e-6, on terms of < 1e-2 rad).
 // PLANAR: every pixel of the tile has dz == 0.
-// WIDE: the records hold w_hat - w0, so the product with d is the small
-// sd = s - s0 (s0 = w0 . d per pixel); the phase is theta + sd + N with
+// WIDE: the records hold w_hat - w0 and theta, so the product with d is the
+// small sd = s - s0 (s0 = w0 . d per pixel); the phase is theta + sd + N with
 // every term small, and only the range bin uses the full s0 + ...:
 // exp(-j s0) is applied in f64 through the final phase.
 template <int MODE, bool PLANAR, bool WIDE, int PPT>
@@ -121,32 +125,39 @@ __device__ __forceinline__ void accumulate(int nc, const PulseRec *__restrict__ 
                                            const float (&s0)[PPT], float (&ar)[PPT], float (&ai)[PPT]) {
 #pragma unroll 2
     for (int i = 0; i < nc; ++i, poff += pstride) {
-        const float4 a = rec[i].a;  // w_hat (or w_hat - w0), e
-        const float4 b = rec[i].b;  // c0, theta, R', bits
-        const float e2 = a.w + a.w;
+        const float4 a = rec[i].a;  // narrow: kappa w_hat, e'; wide: w_hat - w0, e
+        const float4 b = rec[i].b;  // c0, sigma0 (narrow) or theta (wide), R', bits
+        const float ee = a.w * a.w;
+        const float de = -4.0f * ee * b.y;  // e - e' (narrow tiles)
 #pragma unroll
         for (int k = 0; k < PPT; ++k) {
-            float sd = fmaf(a.y, dy[k], a.x * dx[k]);
-            if constexpr (!PLANAR) sd = fmaf(a.z, dz[k], sd);
-            const float s = WIDE ? s0[k] + sd : sd;
-            float D;  // phase argument
-            if constexpr (MODE == 0) {
-                D = fmaf(a.w, fmaf(s, s, nd2[k]), sd) + b.y;
-            } else if constexpr (MODE == 1) {
-                const float t = fmaf(s, s, nd2[k]);
-                D = fmaf(a.w * t, fmaf(e2, s, 1.0f), sd) + b.y;
-            } else if constexpr (MODE == 2) {
-                const float en = a.w * nd2[k];  // h - s
-                const float h = s + en;
-                const float y = a.w * h;
-                const float q = fmaf(y, fmaf(5.0f, y, 2.0f), 1.0f);
-                D = (sd + fmaf(h * y, q, en)) + b.y;
+            float D, s;  // phase argument; s = w_hat . d (approximate for narrow tiles)
+            if constexpr (!WIDE) {
+                float sg = fmaf(a.x, dx[k], b.y);
+                sg = fmaf(a.y, dy[k], sg);
+                if constexpr (!PLANAR) sg = fmaf(a.z, dz[k], sg);
+                D = fmaf(a.w, fmaf(sg, sg, nd2[k]), sg);
+                s = sg - b.y;
+                if constexpr (MODE >= 1) D = fmaf(de, nd2[k], D);
             } else {
+                float sd = fmaf(a.y, dy[k], a.x * dx[k]);
+                if constexpr (!PLANAR) sd = fmaf(a.z, dz[k], sd);
+                s = s0[k] + sd;
+                D = fmaf(a.w, fmaf(s, s, nd2[k]), sd) + b.y;
+            }
+            if constexpr (MODE == 1) {
+                D = fmaf(2.0f * ee * s, fmaf(s, s, nd2[k]), D);
+            } else if constexpr (MODE == 2) {
+                const float h = fmaf(a.w, nd2[k], s);
+                const float q = fmaf(5.0f * a.w, h, 2.0f);
+                D = fmaf(ee, fmaf(h * h * h, q, nd2[k] * (h + s)), D);
+            } else if constexpr (MODE == 3) {
                 const float h = fmaf(a.w, nd2[k], s);
                 const float q = fmaxf(fmaf(-2.0f, h, b.z), 0.0f);
                 const float den = b.z + sqrtf(b.z * q);
                 const float Dn = __fdividef(2.0f * b.z * h, den);
-                D = (sd + __fdividef(fmaf(s, Dn, nd2[k]), den)) + b.y;
+                const float N = __fdividef(fmaf(s, Dn, nd2[k]), den);
+                D += N - a.w * fmaf(s, s, nd2[k]);  // exact nonlinear part less the two-term one
             }
             const float Di = WIDE ? s0[k] + D : D;  // range-bin argument
             float tl = fmaf(Di, ilk, b.x);

@@ -187,14 +187,27 @@ __global__ void __launch_bounds__(kThreadsGeom) pulse_record_kernel(const DevJob
         const float e2 = 2.0f * rk * gm * gm;
         const float e3 = 5.0f * rk * gm * gm * gm;
         const float e4 = 14.0f * rk * gm * gm * gm * gm;
-        const int order = (e4 > kPhaseTol || gm > 5e-3f) ? 3 : e3 > kPhaseTol ? 2 : e2 > kPhaseTol ? 1 : 0;
+        int order = (e4 > kPhaseTol || gm > 5e-3f) ? 3 : e3 > kPhaseTol ? 2 : e2 > kPhaseTol ? 1 : 0;
         const int base = (int)fl - t.K;
-        const double ox = t.wide ? (double)t.w0[0] : 0.0, oy = t.wide ? (double)t.w0[1] : 0.0,
-                     oz = t.wide ? (double)t.w0[2] : 0.0;
-        rec.a = make_float4((float)(wx * iR - ox), (float)(wy * iR - oy), (float)(wz * iR - oz),
-                            (float)(0.5 * iR / k_c));
+        const double e = 0.5 * iR / k_c;
         const double c0 = (tc - fl) + ((double)t.K - 0.5) - theta * (jb.inv_lsr / k_c);
-        rec.b = make_float4((float)c0, (float)theta, (float)(k_c * R), __int_as_float(8 * base + order));
+        if (t.wide) {
+            rec.a = make_float4((float)(wx * iR - (double)t.w0[0]), (float)(wy * iR - (double)t.w0[1]),
+                                (float)(wz * iR - (double)t.w0[2]), (float)e);
+            rec.b = make_float4((float)c0, (float)theta, (float)(k_c * R), __int_as_float(8 * base + order));
+        } else {
+            // theta folded into the linear term: sigma = kappa (w_hat . d + theta)
+            // + e theta^2 with kappa = 1 - 2 e theta, so that theta + s + e t =
+            // sigma + e' (sigma^2 - |d|^2) + (e - e')(-|d|^2), e' = e / kappa^2;
+            // the last term is below 4 pi gm^2 rad and is added from series
+            // order 1 on, which tiles with gm > 4e-4 always use
+            if (gm > 4e-4f) order = max(order, 1);
+            const double kap = 1.0 - 2.0 * e * theta;
+            rec.a = make_float4((float)(kap * wx * iR), (float)(kap * wy * iR), (float)(kap * wz * iR),
+                                (float)(e / (kap * kap)));
+            rec.b = make_float4((float)c0, (float)(kap * theta + e * theta * theta), (float)(k_c * R),
+                                __int_as_float(8 * base + order));
+        }
     } else {
         // no contribution: the staging leaves this pulse's window at zero
         rec.a = make_float4(0.f, 0.f, 0.f, 0.f);
