@@ -326,6 +326,18 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
     constexpr int ROWS = kConsumers / TX;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int lx = tid % TX, ly = tid / TX;
+    // pixel k of this thread: lanes run along x, or along y on transposed
+    // tiles (square tiles whose range bins step faster along x than along y,
+    // so that neighbouring lanes read neighbouring or equal window entries)
+    auto pixel_of = [&](bool tr, int tx0, int ty0, int k, int &ix, int &iy) {
+        if (TX == TY && tr) {
+            ix = tx0 + ly + k * ROWS;
+            iy = ty0 + lx;
+        } else {
+            ix = tx0 + lx;
+            iy = ty0 + ly + k * ROWS;
+        }
+    };
     const uint32_t stage_base = smem_u32(sm.stage) - kMagicOff;
     int item = blockIdx.x;
     for (;;) {
@@ -349,7 +361,8 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
         float dx[PPT], dy[PPT], dz[PPT], nd2[PPT], s0[PPT], ar[PPT], ai[PPT];
 #pragma unroll
         for (int k = 0; k < PPT; ++k) {
-            const int ix = tx0 + lx, iy = ty0 + ly + k * ROWS;
+            int ix, iy;
+            pixel_of(ti.transposed != 0, tx0, ty0, k, ix, iy);
             dx[k] = dy[k] = dz[k] = nd2[k] = s0[k] = ar[k] = ai[k] = 0.0f;
             if (ix < nu && iy < nv) {
                 double x, y, z;
@@ -401,7 +414,8 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
         double zmax = 0.0;
 #pragma unroll
         for (int k = 0; k < PPT; ++k) {
-            const int ix = tx0 + lx, iy = ty0 + ly + k * ROWS;
+            int ix, iy;
+            pixel_of(ti.transposed != 0, tx0, ty0, k, ix, iy);
             if (ix < nu && iy < nv) {
                 const float2 f = jb.fin[(long long)iy * nu + ix];
                 const double zr = (double)fmaf(ar[k], f.x, -ai[k] * f.y);

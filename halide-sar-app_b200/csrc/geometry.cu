@@ -151,7 +151,25 @@ __global__ void __launch_bounds__(kThreadsGeom) tile_setup_kernel(const DevJob *
         t.w0[0] = w0f[0];
         t.w0[1] = w0f[1];
         t.w0[2] = w0f[2];
-        t.pad = 0;
+        // Lane orientation: the window entries that neighbouring lanes read
+        // are |w . step| / lsr bins apart for a one-pixel step; apart by one
+        // or more, eight lanes span more than the eight 16-byte banks of a
+        // shared-memory wavefront and collide.  Run the lanes along the axis
+        // with the smaller step (square tiles only).
+        t.transposed = 0;
+        if (TX == TY && tx0 + 1 < jb.nu && ty0 + 1 < jb.nv) {
+            double x0, y0, z0, x1, y1, z1, x2, y2, z2;
+            pixel_pos(jb, tx0, ty0, x0, y0, z0);
+            pixel_pos(jb, tx0 + 1, ty0, x1, y1, z1);
+            pixel_pos(jb, tx0, ty0 + 1, x2, y2, z2);
+            const double gx = pm.x - rc[0], gy = pm.y - rc[1], gz = pm.z - rc[2];
+            const double g = sqrt(gx * gx + gy * gy + gz * gz);
+            if (g > 0.0 && isfinite(g)) {
+                const double sx = fabs(gx * (x1 - x0) + gy * (y1 - y0) + gz * (z1 - z0)) / (g * jb.lsr);
+                const double sy = fabs(gx * (x2 - x0) + gy * (y2 - y0) + gz * (z2 - z0)) / (g * jb.lsr);
+                if (sx >= 1.0 && sy < sx) t.transposed = 1;
+            }
+        }
         jb.tiles[wi.tile] = t;
         if (bad) atomicOr(&jb.sc->status, kStatusNonFinite);
     }

@@ -45,7 +45,7 @@ struct __align__(16) TileInfo {
     int planar;    // 1 when every pixel has r.z == rc.z
     int wide;      // 1: records hold w_hat - w0, fin carries exp(-j w0 . d)
     float w0[3];   // unit direction from rc to the mid-aperture antenna (wide tiles)
-    int pad;
+    int transposed;  // 1: consumer lanes run along y (square tiles; see tile set-up)
 };
 
 // Per-(tile, pulse) constants (pulse-record kernel -> backprojection):
