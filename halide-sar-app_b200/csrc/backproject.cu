@@ -117,75 +117,112 @@ __device__ __forceinline__ void bulk_copy(void *dst, const void *src, uint32_t b
 // small sd = s - s0 (s0 = w0 . d per pixel); the phase is theta + sd + N with
 // every term small, and only the range bin uses the full s0 + ...:
 // exp(-j s0) is applied in f64 through the final phase.
-template <int MODE, bool PLANAR, bool WIDE, int PPT>
-__device__ __forceinline__ void accumulate(int nc, const PulseRec *__restrict__ rec, uint32_t poff,
-                                           uint32_t pstride, float ilk, float hi_clamp,
-                                           const float (&dx)[PPT], const float (&dy)[PPT],
-                                           const float (&dz)[PPT], const float (&nd2)[PPT],
-                                           const float (&s0)[PPT], float (&ar)[PPT], float (&ai)[PPT]) {
+// Paired form: the consumer's pixels go in pairs through the f32x2
+// instructions of sm_100 (FFMA2/FADD2/FMUL2: two lanes of FP32 per
+// instruction, the same rounding as two scalar operations), so every
+// per-pixel FP32 step up to the range bin costs half an issue slot; the
+// window loads, the interpolation and the sine/cosine stay per pixel.  Each
+// record is staged as four float4 of broadcast pairs (see expand_records).
+// The images are the same bit for bit as with scalar arithmetic.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+template <int MODE, bool PLANAR, bool WIDE, int NP>
+__device__ __forceinline__ void accumulate(int nc, const float4 *__restrict__ rec2, uint32_t poff,
+                                           uint32_t pstride, float2 ILK, float hi_clamp,
+                                           const float2 (&dx)[NP], const float2 (&dy)[NP],
+                                           const float2 (&dz)[NP], const float2 (&nd2)[NP],
+                                           const float2 (&s0)[NP], float2 (&ar)[NP], float2 (&ai)[NP]) {
+    const float2 M2 = f2(kMagic, kMagic), NM2 = f2(-kMagic, -kMagic), NEG1 = f2(-1.0f, -1.0f);
 #pragma unroll 2
     for (int i = 0; i < nc; ++i, poff += pstride) {
-        const float4 a = rec[i].a;  // narrow: kappa w_hat, e'; wide: w_hat - w0, e
-        const float4 b = rec[i].b;  // c0, sigma0 (narrow) or theta (wide), R', bits
-        const float ee = a.w * a.w;
-        const float de = -4.0f * ee * b.y;  // e - e' (narrow tiles)
+        const float4 q0 = rec2[4 * i];      // ax ax ay ay   (narrow: kappa w_hat; wide: w_hat - w0)
+        const float4 q1 = rec2[4 * i + 1];  // az az e  e    (narrow: e')
+        const float4 q2 = rec2[4 * i + 2];  // c0 c0 b  b    (narrow: sigma0; wide: theta)
+        const float2 AX = f2(q0.x, q0.y), AY = f2(q0.z, q0.w), AZ = f2(q1.x, q1.y);
+        const float2 E = f2(q1.z, q1.w), C0 = f2(q2.x, q2.y), B = f2(q2.z, q2.w);
+        float Rp = 0.0f;
+        if constexpr (MODE == 3) Rp = rec2[4 * i + 3].x;
+        const float ee = q1.z * q1.z;
+        const float2 EE = f2(ee, ee);
+        const float de = -4.0f * ee * q2.z;  // e - e' (narrow tiles)
+        const float2 DE = f2(de, de);
 #pragma unroll
-        for (int k = 0; k < PPT; ++k) {
-            float D, s;  // phase argument; s = w_hat . d (approximate for narrow tiles)
+        for (int j = 0; j < NP; ++j) {
+            float2 D, s;  // phase argument; s = w_hat . d (approximate for narrow tiles)
             if constexpr (!WIDE) {
-                float sg = fmaf(a.x, dx[k], b.y);
-                sg = fmaf(a.y, dy[k], sg);
-                if constexpr (!PLANAR) sg = fmaf(a.z, dz[k], sg);
-                D = fmaf(a.w, fmaf(sg, sg, nd2[k]), sg);
-                s = sg - b.y;
-                if constexpr (MODE >= 1) D = fmaf(de, nd2[k], D);
+                float2 sg = __ffma2_rn(AX, dx[j], B);
+                sg = __ffma2_rn(AY, dy[j], sg);
+                if constexpr (!PLANAR) sg = __ffma2_rn(AZ, dz[j], sg);
+                D = __ffma2_rn(E, __ffma2_rn(sg, sg, nd2[j]), sg);
+                s = __ffma2_rn(B, NEG1, sg);
+                if constexpr (MODE >= 1) D = __ffma2_rn(DE, nd2[j], D);
             } else {
-                float sd = fmaf(a.y, dy[k], a.x * dx[k]);
-                if constexpr (!PLANAR) sd = fmaf(a.z, dz[k], sd);
-                s = s0[k] + sd;
-                D = fmaf(a.w, fmaf(s, s, nd2[k]), sd) + b.y;
+                float2 sd = __fmul2_rn(AX, dx[j]);
+                sd = __ffma2_rn(AY, dy[j], sd);
+                if constexpr (!PLANAR) sd = __ffma2_rn(AZ, dz[j], sd);
+                s = __fadd2_rn(s0[j], sd);
+                D = __fadd2_rn(__ffma2_rn(E, __ffma2_rn(s, s, nd2[j]), sd), B);
             }
             if constexpr (MODE == 1) {
-                D = fmaf(2.0f * ee * s, fmaf(s, s, nd2[k]), D);
+                D = __ffma2_rn(__fmul2_rn(__fadd2_rn(EE, EE), s), __ffma2_rn(s, s, nd2[j]), D);
             } else if constexpr (MODE == 2) {
-                const float h = fmaf(a.w, nd2[k], s);
-                const float q = fmaf(5.0f * a.w, h, 2.0f);
-                D = fmaf(ee, fmaf(h * h * h, q, nd2[k] * (h + s)), D);
+                const float2 h = __ffma2_rn(E, nd2[j], s);
+                const float2 q = __ffma2_rn(__fmul2_rn(f2(5.0f, 5.0f), E), h, f2(2.0f, 2.0f));
+                const float2 h3 = __fmul2_rn(__fmul2_rn(h, h), h);
+                D = __ffma2_rn(EE, __ffma2_rn(h3, q, __fmul2_rn(nd2[j], __fadd2_rn(h, s))), D);
             } else if constexpr (MODE == 3) {
-                const float h = fmaf(a.w, nd2[k], s);
-                const float q = fmaxf(fmaf(-2.0f, h, b.z), 0.0f);
-                const float den = b.z + sqrtf(b.z * q);
-                const float Dn = __fdividef(2.0f * b.z * h, den);
-                const float N = __fdividef(fmaf(s, Dn, nd2[k]), den);
-                D += N - a.w * fmaf(s, s, nd2[k]);  // exact nonlinear part less the two-term one
+                float n[2];
+#pragma unroll
+                for (int l = 0; l < 2; ++l) {
+                    const float sl = l ? s.y : s.x, nl = l ? nd2[j].y : nd2[j].x, el = q1.z;
+                    const float h = fmaf(el, nl, sl);
+                    const float q = fmaxf(fmaf(-2.0f, h, Rp), 0.0f);
+                    const float den = Rp + sqrtf(Rp * q);
+                    const float Dn = __fdividef(2.0f * Rp * h, den);
+                    // exact nonlinear part less the two-term one
+                    n[l] = __fdividef(fmaf(sl, Dn, nl), den) - el * fmaf(sl, sl, nl);
+                }
+                D = __fadd2_rn(D, f2(n[0], n[1]));
             }
-            const float Di = WIDE ? s0[k] + D : D;  // range-bin argument
-            float tl = fmaf(Di, ilk, b.x);
-            if constexpr (MODE >= 2) tl = fminf(fmaxf(tl, 0.0f), hi_clamp);
-            const float f = tl + kMagic;
-            const float wgt = tl - (f - kMagic);
-            const uint32_t o = (__float_as_uint(f) << 4) + poff;  // shared-window address
-            float4 md;
+            const float2 Di = WIDE ? __fadd2_rn(s0[j], D) : D;  // range-bin argument
+            float2 tl = __ffma2_rn(Di, ILK, C0);
+            if constexpr (MODE >= 2) {
+                tl.x = fminf(fmaxf(tl.x, 0.0f), hi_clamp);
+                tl.y = fminf(fmaxf(tl.y, 0.0f), hi_clamp);
+            }
+            const float2 f = __fadd2_rn(tl, M2);
+            const float2 w = __ffma2_rn(__fadd2_rn(f, NM2), NEG1, tl);  // tl - floor(tl)
+            float4 m0, m1;
+            const uint32_t o0 = (__float_as_uint(f.x) << 4) + poff;  // shared-window addresses
+            const uint32_t o1 = (__float_as_uint(f.y) << 4) + poff;
             asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
-                         : "=f"(md.x), "=f"(md.y), "=f"(md.z), "=f"(md.w)
-                         : "r"(o));
-            const float vr = fmaf(wgt, md.z, md.x);
-            const float vi = fmaf(wgt, md.w, md.y);
-            float sn, cs;
-            __sincosf(D, &sn, &cs);
-            ar[k] = fmaf(vr, cs, fmaf(vi, sn, ar[k]));
-            ai[k] = fmaf(vi, cs, fmaf(-vr, sn, ai[k]));
+                         : "=f"(m0.x), "=f"(m0.y), "=f"(m0.z), "=f"(m0.w)
+                         : "r"(o0));
+            asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                         : "=f"(m1.x), "=f"(m1.y), "=f"(m1.z), "=f"(m1.w)
+                         : "r"(o1));
+            const float vr0 = fmaf(w.x, m0.z, m0.x), vi0 = fmaf(w.x, m0.w, m0.y);
+            const float vr1 = fmaf(w.y, m1.z, m1.x), vi1 = fmaf(w.y, m1.w, m1.y);
+            float sn0, cs0, sn1, cs1;
+            __sincosf(D.x, &sn0, &cs0);
+            __sincosf(D.y, &sn1, &cs1);
+            const float2 VR = f2(vr0, vr1), VI = f2(vi0, vi1), SN = f2(sn0, sn1), CS = f2(cs0, cs1);
+            ar[j] = __ffma2_rn(VR, CS, __ffma2_rn(VI, SN, ar[j]));
+            float2 t = __ffma2_rn(VI, CS, ai[j]);
+            t.x = fmaf(-vr0, sn0, t.x);
+            t.y = fmaf(-vr1, sn1, t.y);
+            ai[j] = t;
         }
     }
 }
 
-template <bool WIDE, int PPT>
-__device__ __forceinline__ void accumulate_mode(int mode, bool planar, int nc, const PulseRec *rec,
-                                                uint32_t poff, uint32_t pstride, float ilk, float hi,
-                                                const float (&dx)[PPT], const float (&dy)[PPT],
-                                                const float (&dz)[PPT], const float (&nd2)[PPT],
-                                                const float (&s0)[PPT], float (&ar)[PPT], float (&ai)[PPT]) {
-#define SARBP_ACC(M, PL) accumulate<M, PL, WIDE, PPT>(nc, rec, poff, pstride, ilk, hi, dx, dy, dz, nd2, s0, ar, ai)
+template <bool WIDE, int NP>
+__device__ __forceinline__ void accumulate_mode(int mode, bool planar, int nc, const float4 *rec2,
+                                                uint32_t poff, uint32_t pstride, float2 ILK, float hi,
+                                                const float2 (&dx)[NP], const float2 (&dy)[NP],
+                                                const float2 (&dz)[NP], const float2 (&nd2)[NP],
+                                                const float2 (&s0)[NP], float2 (&ar)[NP], float2 (&ai)[NP]) {
+#define SARBP_ACC(M, PL) accumulate<M, PL, WIDE, NP>(nc, rec2, poff, pstride, ILK, hi, dx, dy, dz, nd2, s0, ar, ai)
     if (mode == 0) {
         if (planar) SARBP_ACC(0, true);
         else SARBP_ACC(0, false);
@@ -204,7 +241,8 @@ __device__ __forceinline__ void accumulate_mode(int mode, bool planar, int nc, c
 // Shared memory of the tile kernel.
 struct TileSmem {
     float4 *stage;       // [2][stage_cap] (m, d) windows
-    PulseRec *rec;       // [2][cmax]
+    PulseRec *raw;       // [cmax] records as copied (producer only)
+    float4 *rec2;        // [2][4 cmax] records as broadcast pairs (see accumulate)
     uint64_t *mbar_rec;  // [2]
     uint64_t *mbar_win;  // [2]
     double *sred;        // [kConsumerWarps]
@@ -232,7 +270,7 @@ __device__ __forceinline__ bool stage_chunk(const DevJob &jb, int tile, int lane
                                             const TileShape &sh, int stage_cap, int cmax,
                                             const TileSmem &sm, uint32_t (&uses)[4]) {
     const int N = jb.N, W = sh.W;
-    PulseRec *rec = sm.rec + b * cmax;
+    PulseRec *rec = sm.raw;
     float4 *win = sm.stage + b * stage_cap;
     // prior generic-proxy reads of these buffers come before the async writes
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -243,6 +281,15 @@ __device__ __forceinline__ bool stage_chunk(const DevJob &jb, int tile, int lane
     }
     bool ok = mbar_wait(&sm.mbar_rec[b], uses[b] & 1u);
     uses[b]++;
+    // records as the consumers read them: four float4 of broadcast pairs
+    float4 *r2 = sm.rec2 + (size_t)b * 4 * cmax;
+    for (int i = lane; i < nc; i += 32) {
+        const float4 a = rec[i].a, q = rec[i].b;
+        r2[4 * i] = make_float4(a.x, a.x, a.y, a.y);
+        r2[4 * i + 1] = make_float4(a.z, a.z, a.w, a.w);
+        r2[4 * i + 2] = make_float4(q.x, q.x, q.y, q.y);
+        r2[4 * i + 3] = make_float4(q.z, q.w, 0.0f, 0.0f);
+    }
     // window copies: bins [base, base + W) of row p; the in-profile part
     // [max(base, 0), min(base + W, N)) comes from the pairs row
     uint32_t bytes = 0;
@@ -358,12 +405,12 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
         const float kcf = (float)k_c;
 
         // ---- pixel offsets from the tile centre, in radians ----
-        float dx[PPT], dy[PPT], dz[PPT], nd2[PPT], s0[PPT], ar[PPT], ai[PPT];
+        float dx[PPT], dy[PPT], dz[PPT], nd2[PPT], s0[PPT];
 #pragma unroll
         for (int k = 0; k < PPT; ++k) {
             int ix, iy;
             pixel_of(ti.transposed != 0, tx0, ty0, k, ix, iy);
-            dx[k] = dy[k] = dz[k] = nd2[k] = s0[k] = ar[k] = ai[k] = 0.0f;
+            dx[k] = dy[k] = dz[k] = nd2[k] = s0[k] = 0.0f;
             if (ix < nu && iy < nv) {
                 double x, y, z;
                 if (jb.r) {
@@ -389,10 +436,23 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
                 }
             }
         }
+        // pixel pairs (2j, 2j + 1) for the f32x2 arithmetic
+        constexpr int NP = PPT / 2;
+        float2 dxp[NP], dyp[NP], dzp[NP], nd2p[NP], s0p[NP], arp[NP], aip[NP];
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+            dxp[j] = make_float2(dx[2 * j], dx[2 * j + 1]);
+            dyp[j] = make_float2(dy[2 * j], dy[2 * j + 1]);
+            dzp[j] = make_float2(dz[2 * j], dz[2 * j + 1]);
+            nd2p[j] = make_float2(nd2[2 * j], nd2[2 * j + 1]);
+            s0p[j] = make_float2(s0[2 * j], s0[2 * j + 1]);
+            arp[j] = aip[j] = make_float2(0.0f, 0.0f);
+        }
         if (sh.C < 1) {
             if (tid == 0) atomicOr(&jb.sc->status, kStatusTileTooWide);
         } else {
             const float ilk = (float)(jb.inv_lsr / k_c);  // range bins per radian of Delta
+            const float2 ILK = make_float2(ilk, ilk);
             const float hi = (float)(sh.W - 1) - 0.5f;
             const uint32_t pstride = (uint32_t)sh.W * 16u;
             for (int c = 0; c < sh.nchunks; ++c) {
@@ -401,12 +461,13 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
                 const int p0 = c * sh.C;
                 const uint32_t poff = stage_base + (uint32_t)(b * stage_cap) * 16u;
                 const int nc = min(sh.C, P - p0);
+                const float4 *rec2 = sm.rec2 + (size_t)b * 4 * cmax;
                 if (ti.wide)
-                    accumulate_mode<true, PPT>(sm.s_mode[b], ti.planar != 0, nc, sm.rec + b * cmax, poff,
-                                               pstride, ilk, hi, dx, dy, dz, nd2, s0, ar, ai);
+                    accumulate_mode<true, NP>(sm.s_mode[b], ti.planar != 0, nc, rec2, poff, pstride, ILK, hi,
+                                              dxp, dyp, dzp, nd2p, s0p, arp, aip);
                 else
-                    accumulate_mode<false, PPT>(sm.s_mode[b], ti.planar != 0, nc, sm.rec + b * cmax, poff,
-                                                pstride, ilk, hi, dx, dy, dz, nd2, s0, ar, ai);
+                    accumulate_mode<false, NP>(sm.s_mode[b], ti.planar != 0, nc, rec2, poff, pstride, ILK, hi,
+                                               dxp, dyp, dzp, nd2p, s0p, arp, aip);
                 bar_arrive(kBarEmpty0 + b);
             }
         }
@@ -418,8 +479,10 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
             pixel_of(ti.transposed != 0, tx0, ty0, k, ix, iy);
             if (ix < nu && iy < nv) {
                 const float2 f = jb.fin[(long long)iy * nu + ix];
-                const double zr = (double)fmaf(ar[k], f.x, -ai[k] * f.y);
-                const double zi = (double)fmaf(ar[k], f.y, ai[k] * f.x);
+                const float ark = (k & 1) ? arp[k >> 1].y : arp[k >> 1].x;
+                const float aik = (k & 1) ? aip[k >> 1].y : aip[k >> 1].x;
+                const double zr = (double)fmaf(ark, f.x, -aik * f.y);
+                const double zi = (double)fmaf(ark, f.y, aik * f.x);
                 jb.out[(long long)(nv - 1 - iy) * nu + ix] = make_double2(zr, zi);
                 zmax = fmax(zmax, sqrt(zr * zr + zi * zi));
             }
@@ -444,14 +507,15 @@ __global__ void __launch_bounds__(kThreads, MINB) bp_tile_kernel(const DevJob *_
                                                                  const WorkItem *__restrict__ items,
                                                                  int nitems, int *__restrict__ counter,
                                                                  int stage_cap, int cmax, int persistent) {
-    static_assert(TX * TY % kConsumers == 0, "tile must be a multiple of the consumers");
+    static_assert(TX * TY % (2 * kConsumers) == 0, "tile must give each consumer pairs of pixels");
     extern __shared__ float4 smem[];
     __shared__ double sred[kConsumerWarps];
     __shared__ int s_item, s_mode[2];
     __shared__ uint64_t mbar[4];
     TileSmem sm;
     sm.stage = smem;
-    sm.rec = reinterpret_cast<PulseRec *>(smem + 2 * stage_cap);
+    sm.raw = reinterpret_cast<PulseRec *>(smem + 2 * stage_cap);
+    sm.rec2 = smem + 2 * stage_cap + 2 * cmax;
     sm.mbar_rec = mbar;
     sm.mbar_win = mbar + 2;
     sm.sred = sred;
@@ -533,9 +597,10 @@ int active_blocks(size_t smem) {
 }  // namespace
 
 // (tile width, tile height, CTAs per SM) instantiations of bp_tile_kernel
-#define SARBP_BP_TILES(X)                                                                      \
-    X(32, 8, 2) X(32, 16, 2) X(32, 32, 2) X(32, 64, 2) X(64, 16, 2) X(64, 32, 2) X(16, 16, 2)      \
-    X(16, 32, 2) X(16, 64, 2) X(32, 8, 3) X(32, 16, 3) X(32, 32, 3) X(64, 16, 3) X(16, 32, 3)
+// tiles of an even number of pixels per consumer thread (pairs)
+#define SARBP_BP_TILES(X)                                                                  \
+    X(32, 16, 2) X(32, 32, 2) X(32, 64, 2) X(64, 16, 2) X(64, 32, 2) X(16, 32, 2) X(16, 64, 2) \
+    X(32, 16, 3) X(32, 32, 3) X(64, 16, 3) X(16, 32, 3)
 
 bool bp_tile_supported(int tx, int ty, int minb) {
 #define X(a, b, m) \
@@ -546,7 +611,8 @@ bool bp_tile_supported(int tx, int ty, int minb) {
 }
 
 size_t bp_smem_bytes(const BpLaunch &L) {
-    return 2 * (size_t)L.stage_cap * sizeof(float4) + 2 * (size_t)L.cmax * sizeof(PulseRec);
+    return 2 * (size_t)L.stage_cap * sizeof(float4) + (size_t)L.cmax * sizeof(PulseRec) +
+           8 * (size_t)L.cmax * sizeof(float4);
 }
 
 cudaError_t init_backproject_attributes() {

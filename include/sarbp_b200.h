@@ -58,8 +58,8 @@ typedef struct sarbp_ctx sarbp_ctx;
 /* Kernel tuning; a zero field means "library default / autotuned". */
 typedef struct sarbp_opts {
     int precision;   /* SARBP_PREC_* */
-    int tile_x;      /* pixel tile width  (8, 16, 32 or 64) */
-    int tile_y;      /* pixel tile height (must give tile_x*tile_y in {256..4096}) */
+    int tile_x;      /* pixel tile width  (16, 32 or 64) */
+    int tile_y;      /* pixel tile height (tile_x*tile_y in {512, 1024, 2048}) */
     int pulse_chunk; /* pulses staged per chunk (4..256) */
     int persistent;  /* 0 or 1: persistent work-list launch; 2: one CTA per tile */
     int stage_cap;   /* float4 entries of each half of the range-window staging buffer */
