@@ -104,21 +104,24 @@ int run_host_job(sarbp_ctx *ctx, const float *phs, int S, int P, const float *k_
     }
     SlabSpec spec;
     if (nslabs) {
-        if ((e = cudaEventRecord(ctx->ev_in, cin)) != cudaSuccess ||
-            (e = cudaStreamWaitEvent(st, ctx->ev_in, 0)) != cudaSuccess)
-            return cuda_fail(e, "ordering input copies");
-        for (int g = 0; g < nslabs && r; ++g) {
-            const size_t y0 = (size_t)g * slab_rows * tile_y;
-            const size_t y1 = std::min((size_t)nv, (size_t)(g + 1) * slab_rows * tile_y);
-            for (int c = 0; c < 3 && y1 > y0; ++c) {
-                const size_t off = (size_t)c * npix + y0 * (size_t)nu;
-                e = cudaMemcpyAsync(d_r + off, r + off, (y1 - y0) * (size_t)nu * sizeof(double),
-                                    cudaMemcpyHostToDevice, cin);
-                if (e != cudaSuccess) return cuda_fail(e, "copying pixel positions to the device");
+        spec.copy_stream = cin;  // descriptors after the phase history, before the positions
+        // the pixel positions go up slab by slab once the batch's descriptors
+        // and range compression are enqueued (see SlabSpec::before_slabs)
+        spec.before_slabs = [&]() -> cudaError_t {
+            for (int g = 0; g < nslabs && r; ++g) {
+                const size_t y0 = (size_t)g * slab_rows * tile_y;
+                const size_t y1 = std::min((size_t)nv, (size_t)(g + 1) * slab_rows * tile_y);
+                for (int c = 0; c < 3 && y1 > y0; ++c) {
+                    const size_t off = (size_t)c * npix + y0 * (size_t)nu;
+                    cudaError_t ce = cudaMemcpyAsync(d_r + off, r + off, (y1 - y0) * (size_t)nu * sizeof(double),
+                                                     cudaMemcpyHostToDevice, cin);
+                    if (ce != cudaSuccess) return ce;
+                }
+                cudaError_t ce = cudaEventRecord(ctx->ev_ready[g], cin);
+                if (ce != cudaSuccess) return ce;
             }
-            if ((e = cudaEventRecord(ctx->ev_ready[g], cin)) != cudaSuccess)
-                return cuda_fail(e, "cudaEventRecord");
-        }
+            return cudaSuccess;
+        };
         spec.nslabs = nslabs;
         spec.tile_rows = slab_rows;
         spec.aux = ctx->aux;
@@ -222,8 +225,7 @@ int sarbp_ctx_create(int device, sarbp_ctx **out) {
     ctx->stream = ctx->own_stream;
     for (cudaStream_t *sp : {&ctx->copy_in, &ctx->aux, &ctx->copy_out})
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(sp, cudaStreamNonBlocking);
-    for (cudaEvent_t *ev : {&ctx->ev_in, &ctx->ev_out})
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_out, cudaEventDisableTiming);
     for (int g = 0; g < sarbp_ctx::kMaxSlabs && e == cudaSuccess; ++g) {
         e = cudaEventCreateWithFlags(&ctx->ev_ready[g], cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_done[g], cudaEventDisableTiming);
@@ -247,8 +249,7 @@ int sarbp_ctx_destroy(sarbp_ctx *ctx) {
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     for (cudaStream_t sp : {ctx->copy_in, ctx->aux, ctx->copy_out})
         if (sp) cudaStreamDestroy(sp);
-    for (cudaEvent_t ev : {ctx->ev_in, ctx->ev_out})
-        if (ev) cudaEventDestroy(ev);
+    if (ctx->ev_out) cudaEventDestroy(ctx->ev_out);
     for (int g = 0; g < sarbp_ctx::kMaxSlabs; ++g) {
         if (ctx->ev_ready[g]) cudaEventDestroy(ctx->ev_ready[g]);
         if (ctx->ev_done[g]) cudaEventDestroy(ctx->ev_done[g]);

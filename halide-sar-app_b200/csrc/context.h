@@ -22,7 +22,7 @@ struct sarbp_ctx {
     // and the events that pipeline row slabs between them
     static constexpr int kMaxSlabs = 8;
     cudaStream_t copy_in = nullptr, aux = nullptr, copy_out = nullptr;
-    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    cudaEvent_t ev_out = nullptr;
     cudaEvent_t ev_ready[kMaxSlabs] = {}, ev_done[kMaxSlabs] = {};
 };
 

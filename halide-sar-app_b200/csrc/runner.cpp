@@ -414,10 +414,12 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
     }
     std::memcpy(h + o_items, items.data(), items.size() * sizeof(WorkItem));
 
-    e = cudaMemcpyAsync(d, h, meta_bytes, cudaMemcpyHostToDevice, st);
+    cudaStream_t ms = (slabs && slabs->copy_stream) ? slabs->copy_stream : st;
+    e = cudaMemcpyAsync(d, h, meta_bytes, cudaMemcpyHostToDevice, ms);
     if (e != cudaSuccess) return cuda_fail(e, "copying descriptors");
-    e = for_graph ? cudaSuccess : cudaEventRecord(meta_done_, st);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    e = for_graph ? cudaSuccess : cudaEventRecord(meta_done_, ms);
+    if (e == cudaSuccess && ms != st) e = cudaStreamWaitEvent(st, meta_done_, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "ordering the descriptor copy");
 
     const DevJob *d_jobs = reinterpret_cast<const DevJob *>(d + o_jobs);
     const RowItem *d_rows = reinterpret_cast<const RowItem *>(d + o_rows);
@@ -458,6 +460,8 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         return SARBP_OK;
     }
     const bool slabbed = slabs && !items.empty() && prec[0] != SARBP_PREC_NAIVE;
+    if (slabs && slabs->before_slabs && (e = slabs->before_slabs()) != cudaSuccess)
+        return cuda_fail(e, "slab input copies");
     if (slabbed) {
         // ---- row slabs: geometry + backprojection per slab, two streams ----
         if ((e = cudaEventRecord(front_done_, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <string>
@@ -74,6 +75,18 @@ struct SlabSpec {
     cudaStream_t aux = nullptr;
     const cudaEvent_t *ready = nullptr;  // [nslabs] or NULL
     const cudaEvent_t *done = nullptr;   // [nslabs]
+    // Called once the descriptors and the range compression are enqueued and
+    // before any slab waits on `ready`: the place to issue the slabs' input
+    // copies and record `ready`.  Host-to-device copies of all streams share
+    // the copy engine in issue order, so copies issued earlier would hold
+    // back the batch's own descriptor upload.
+    std::function<cudaError_t()> before_slabs;
+    // When set, the batch's descriptors are uploaded on this stream (where
+    // the caller has already queued the phase-history copies) and the
+    // kernels wait for them there: the copy engine runs one stream's queue
+    // ahead of another's, so a descriptor copy on the compute stream could
+    // wait behind every queued input copy.
+    cudaStream_t copy_stream = nullptr;
 };
 
 class Runner {
