@@ -11,9 +11,11 @@
 // all the batch's tiles) and the copies of the images back to the host, and
 // frees the request memory stream-ordered behind them.  Requests that arrive
 // while other batches are on the GPU go into the next free lane, so batches
-// of different lanes overlap on the device.  A completion thread waits for
-// the lanes' batches in launch order, stamps the requests done and returns
-// their budget.
+// of different lanes overlap on the device.  A completion thread picks up
+// the lanes' batches in whichever order they finish, stamps the requests
+// done and returns their budget.  A batch holds at most max_batch requests
+// and max_work pixel*pulses, which bounds how long a small request can wait
+// for the large ones it shares a batch with.
 //
 // Footprint of a request: its device inputs and outputs plus its share of
 // its batch's scratch, all taken from the server's memory pool when the
@@ -97,7 +99,7 @@ struct sarbp_server {
     sarbp_opts launch{};
     size_t cap = 0;
     int max_batch = 32;
-    double max_work = 4e10;  // pixel*pulses per batch (bounds a batch's latency)
+    double max_work = 1.2e10;  // pixel*pulses per batch (bounds a batch's latency)
     cudaMemPool_t pool = nullptr;
     Clock::time_point t0 = Clock::now();
 
@@ -268,14 +270,25 @@ void sarbp_server::completer() {
     for (;;) {
         cv.wait(lk, [&] { return !inflight.empty() || sched_exited; });
         if (inflight.empty()) return;
-        Lane &L = *inflight.front();
+        // the first lane whose batch is done (batches of different lanes
+        // finish out of launch order: a small one need not wait for a large one)
+        Lane *L = nullptr;
+        for (Lane *c : inflight)
+            if (cudaEventQuery(c->done) != cudaErrorNotReady) {
+                L = c;
+                break;
+            }
+        if (!L) {
+            cv.wait_for(lk, std::chrono::microseconds(50));
+            continue;
+        }
         lk.unlock();
-        cudaError_t e = cudaEventSynchronize(L.done);
-        int rc = e == cudaSuccess ? L.runner->check_status(L.st) : cuda_fail(e, "serving: waiting for a batch");
+        cudaError_t e = cudaEventSynchronize(L->done);
+        int rc = e == cudaSuccess ? L->runner->check_status(L->st) : cuda_fail(e, "serving: waiting for a batch");
         std::string err = rc ? last_error_cstr() : std::string();
         const double t = now();
         lk.lock();
-        for (Request *q : L.batch) {
+        for (Request *q : L->batch) {
             if (q->status == SARBP_OK && rc) {
                 q->status = rc;
                 q->error = err;
@@ -284,11 +297,11 @@ void sarbp_server::completer() {
             q->done = true;
             ++completed;
         }
-        in_use -= L.charged;
-        L.charged = 0;
-        L.batch.clear();
-        L.busy = false;
-        inflight.pop_front();
+        in_use -= L->charged;
+        L->charged = 0;
+        L->batch.clear();
+        L->busy = false;
+        inflight.erase(std::find(inflight.begin(), inflight.end(), L));
         cv.notify_all();
     }
 }
@@ -296,7 +309,7 @@ void sarbp_server::completer() {
 extern "C" {
 
 int sarbp_server_create(sarbp_ctx *ctx, const sarbp_opts *launch, double hbm_cap_bytes, int lanes,
-                        int max_batch, sarbp_server **out) {
+                        int max_batch, double max_batch_work, sarbp_server **out) {
     int rc = ctx_set_device(ctx);
     if (rc) return rc;
     if (!out) return fail(SARBP_ERR_INVALID, "out is NULL");
@@ -307,6 +320,7 @@ int sarbp_server_create(sarbp_ctx *ctx, const sarbp_opts *launch, double hbm_cap
     if (launch) s->launch = *launch;
     s->cap = (size_t)hbm_cap_bytes;
     s->max_batch = max_batch > 0 ? max_batch : 32;
+    if (max_batch_work > 0) s->max_work = max_batch_work;
     const int nl = lanes > 0 ? std::min(lanes, 8) : 2;
     cudaMemPoolProps props{};
     props.allocType = cudaMemAllocationTypePinned;

@@ -265,11 +265,12 @@ class Server:
     (ERR_TIMEOUT while in flight); times(id) gives (submit, start, done)
     seconds on the server's clock."""
 
-    def __init__(self, ctx, hbm_cap_bytes=150e9, lanes=2, max_batch=32, precision=None, **tune):
+    def __init__(self, ctx, hbm_cap_bytes=150e9, lanes=2, max_batch=32, max_batch_work=0.0,
+                 precision=None, **tune):
         o = _opts(precision, **tune)
         self._h = ctypes.c_void_p()
         check(lib().sarbp_server_create(ctx._h, ctypes.byref(o), float(hbm_cap_bytes), int(lanes),
-                                        int(max_batch), ctypes.byref(self._h)))
+                                        int(max_batch), float(max_batch_work), ctypes.byref(self._h)))
         self._keep = {}
 
     def submit(self, job, keep=None):

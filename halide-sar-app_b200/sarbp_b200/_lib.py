@@ -85,7 +85,8 @@ SIGNATURES = {
     "sarbp_plan_kernel_count": (ctypes.c_int, [ctypes.c_void_p]),
     "sarbp_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "sarbp_server_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Opts), ctypes.c_double,
-                                           ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+                                           ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                           ctypes.POINTER(ctypes.c_void_p)]),
     "sarbp_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job),
                                            ctypes.POINTER(ctypes.c_longlong)]),
     "sarbp_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double]),

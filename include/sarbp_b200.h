@@ -201,8 +201,10 @@ int sarbp_plan_destroy(sarbp_plan *plan);
  * requests in arrival order while their device footprint (inputs, outputs,
  * and their batch's scratch) fits hbm_cap_bytes, uploads each phase history
  * once, and launches them as one batch on the first free of `lanes` streams
- * (default 2), at most max_batch requests per batch (default 32); batches of
- * different lanes overlap on the device.  A request that cannot fit an idle
+ * (default 2), at most max_batch requests (default 32) and max_batch_work
+ * pixel*pulses (default 1.2e10, about 10 ms of work) per batch; batches of
+ * different lanes overlap on the device and complete in whichever order
+ * they finish.  A request that cannot fit an idle
  * server fails with SARBP_ERR_ADMISSION.  `launch` (may be NULL) fixes the
  * precision and launch shape of every batch, so a request's image does not
  * depend on what it was batched with.
@@ -210,7 +212,7 @@ int sarbp_plan_destroy(sarbp_plan *plan);
 typedef struct sarbp_server sarbp_server;
 int sarbp_server_create(sarbp_ctx *ctx, const sarbp_opts *launch,
                         double hbm_cap_bytes, int lanes, int max_batch,
-                        sarbp_server **out);
+                        double max_batch_work, sarbp_server **out);
 int sarbp_server_submit(sarbp_server *server, const sarbp_job *host_job,
                         long long *id);
 /* Waits up to timeout_s (< 0: no limit) for request id; returns its status,
