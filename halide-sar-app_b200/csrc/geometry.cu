@@ -45,37 +45,42 @@ __device__ __forceinline__ void pixel_pos(const DevJob &jb, int ix, int iy, doub
     }
 }
 
-template <class T, class Op>
-__device__ T block_reduce(T v, T *sbuf, Op op) {
-    for (int o = 16; o > 0; o >>= 1) v = op(v, __shfl_xor_sync(0xffffffffu, v, o));
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __syncthreads();
-    if (lane == 0) sbuf[warp] = v;
-    __syncthreads();
-    v = sbuf[0];
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) v = op(v, sbuf[w]);
+
+// pixels per thread of the largest tile (2048 pixels, 256 threads)
+constexpr int kGeomPix = 8;
+
+__device__ __forceinline__ double warp_min_d(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_max_d(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
 }
 
-struct MinOp { __device__ double operator()(double a, double b) const { return fmin(a, b); } };
-struct MaxOp { __device__ double operator()(double a, double b) const { return fmax(a, b); } };
-struct MaxOpF { __device__ float operator()(float a, float b) const { return fmaxf(a, b); } };
-struct AndOp { __device__ int operator()(int a, int b) const { return a & b; } };
-struct OrOp { __device__ int operator()(int a, int b) const { return a | b; } };
-
 __global__ void __launch_bounds__(kThreadsGeom) tile_setup_kernel(const DevJob *__restrict__ jobs,
                                                                   const WorkItem *__restrict__ items) {
-    __shared__ double sd[32];
-    __shared__ float sf[32];
-    __shared__ int si[32];
+    constexpr int kWarps = kThreadsGeom / 32;
+    __shared__ double sbox[kWarps][6];
+    __shared__ float srho[kWarps];
+    __shared__ int sflags[kWarps][2];
     const WorkItem wi = items[blockIdx.x];
     const DevJob &jb = jobs[wi.job];
     const int TX = jb.tile_x, TY = jb.tile_y;
+    const int lx = __ffs(TX) - 1;  // tile widths are powers of two
     const int tx0 = (wi.tile % jb.tiles_x) * TX, ty0 = (wi.tile / jb.tiles_x) * TY;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // this thread's pixels, kept in registers for both passes
+    double px[kGeomPix], py[kGeomPix], pz[kGeomPix];
+    unsigned live = 0u;  // bit k: pixel k is inside the image and finite
     double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
     int bad = 0;
-    for (int idx = threadIdx.x; idx < TX * TY; idx += blockDim.x) {
-        const int ix = tx0 + idx % TX, iy = ty0 + idx / TX;
+#pragma unroll
+    for (int k = 0; k < kGeomPix; ++k) {
+        px[k] = py[k] = pz[k] = 0.0;
+        const int idx = threadIdx.x + k * kThreadsGeom;
+        if (idx >= TX * TY) continue;
+        const int ix = tx0 + (idx & (TX - 1)), iy = ty0 + (idx >> lx);
         if (ix >= jb.nu || iy >= jb.nv) continue;
         double x, y, z;
         pixel_pos(jb, ix, iy, x, y, z);
@@ -83,13 +88,33 @@ __global__ void __launch_bounds__(kThreadsGeom) tile_setup_kernel(const DevJob *
             bad = 1;
             continue;
         }
+        px[k] = x;
+        py[k] = y;
+        pz[k] = z;
+        live |= 1u << k;
         mn[0] = fmin(mn[0], x); mx[0] = fmax(mx[0], x);
         mn[1] = fmin(mn[1], y); mx[1] = fmax(mx[1], y);
         mn[2] = fmin(mn[2], z); mx[2] = fmax(mx[2], z);
     }
+    // bounding box: one pass through shared memory for all six extrema
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        mn[d] = warp_min_d(mn[d]);
+        mx[d] = warp_max_d(mx[d]);
+    }
+    if (lane == 0)
+        for (int d = 0; d < 3; ++d) {
+            sbox[warp][d] = mn[d];
+            sbox[warp][3 + d] = mx[d];
+        }
+    __syncthreads();
     double rc[3], hd2 = 0.0;
     for (int d = 0; d < 3; ++d) {
-        const double a = block_reduce(mn[d], sd, MinOp()), b = block_reduce(mx[d], sd, MaxOp());
+        double a = sbox[0][d], b = sbox[0][3 + d];
+        for (int w = 1; w < kWarps; ++w) {
+            a = fmin(a, sbox[w][d]);
+            b = fmax(b, sbox[w][3 + d]);
+        }
         rc[d] = a <= b ? 0.5 * (a + b) : 0.0;
         if (a <= b) hd2 += 0.25 * (b - a) * (b - a);
     }
@@ -111,13 +136,15 @@ __global__ void __launch_bounds__(kThreadsGeom) tile_setup_kernel(const DevJob *
     }
     float rho = 0.0f;
     int planar = 1;
-    for (int idx = threadIdx.x; idx < TX * TY; idx += blockDim.x) {
-        const int ix = tx0 + idx % TX, iy = ty0 + idx / TX;
+#pragma unroll
+    for (int k = 0; k < kGeomPix; ++k) {
+        const int idx = threadIdx.x + k * kThreadsGeom;
+        if (idx >= TX * TY) continue;
+        const int ix = tx0 + (idx & (TX - 1)), iy = ty0 + (idx >> lx);
         if (ix >= jb.nu || iy >= jb.nv) continue;
-        double x, y, z;
-        pixel_pos(jb, ix, iy, x, y, z);
+        const double x = px[k], y = py[k], z = pz[k];
         float2 f = make_float2(0.f, 0.f);
-        if (isfinite(x) && isfinite(y) && isfinite(z)) {
+        if (live & (1u << k)) {
             const float ox = (float)(x - rc[0]), oy = (float)(y - rc[1]), oz = (float)(z - rc[2]);
             rho = fmaxf(rho, sqrtf(fmaf(ox, ox, fmaf(oy, oy, oz * oz))));
             planar &= (oz == 0.0f);
@@ -136,10 +163,23 @@ __global__ void __launch_bounds__(kThreadsGeom) tile_setup_kernel(const DevJob *
         }
         jb.fin[(long long)iy * jb.nu + ix] = f;
     }
-    rho = block_reduce(rho, sf, MaxOpF());
-    planar = block_reduce(planar, si, AndOp());
-    bad = block_reduce(bad, si, OrOp());
+    for (int o = 16; o > 0; o >>= 1) {
+        rho = fmaxf(rho, __shfl_xor_sync(0xffffffffu, rho, o));
+        planar &= __shfl_xor_sync(0xffffffffu, planar, o);
+        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    if (lane == 0) {
+        srho[warp] = rho;
+        sflags[warp][0] = planar;
+        sflags[warp][1] = bad;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
+        for (int w = 1; w < kWarps; ++w) {
+            rho = fmaxf(rho, srho[w]);
+            planar &= sflags[w][0];
+            bad |= sflags[w][1];
+        }
         TileInfo t;
         t.rc[0] = rc[0];
         t.rc[1] = rc[1];
@@ -186,14 +226,15 @@ __global__ void __launch_bounds__(kThreadsGeom) pulse_record_kernel(const DevJob
     const double k_c = jb.sc->k_c;
     const double4 g = jb.pulse[p];
     const double wx = g.x - t.rc[0], wy = g.y - t.rc[1], wz = g.z - t.rc[2];
-    const double R = sqrt(wx * wx + wy * wy + wz * wz);
+    const double R2 = wx * wx + wy * wy + wz * wz;
+    const double iR = rsqrt(R2);  // 1/R and R from one reciprocal square root
+    const double R = R2 * iR;
     const double drc = g.w - R;
     double tc = (drc - jb.lsa) * jb.inv_lsr;
     tc = fmin(fmax(tc, -1.0e8), 1.0e8);
     const double fl = floor(tc);
     PulseRec rec;
     if (isfinite(R) && R > 0.0 && isfinite(tc)) {
-        const double iR = 1.0 / R;
         double th = drc * (k_c * kInv2Pi);
         th = th - rint(th);
         const double theta = kTwoPi * th;  // in [-pi, pi]

@@ -464,6 +464,8 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         return cuda_fail(e, "slab input copies");
     if (slabbed) {
         // ---- row slabs: geometry + backprojection per slab, two streams ----
+        // (stage events: the slabs' geometry counts with the backprojection)
+        if ((e = rec(3)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
         if ((e = cudaEventRecord(front_done_, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
         const int tiles_x = (jobs[0].nu + L.tile_x - 1) / L.tile_x;
         if (bp_max_active_blocks(L) < 1) return fail(SARBP_ERR_CUDA, "backprojection kernel does not fit on an SM");
@@ -504,7 +506,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         if (e != cudaSuccess) return cuda_fail(e, "tile geometry launch");
         dev_->launches += 2;
     }
-    if ((e = rec(3)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    if (!slabbed && (e = rec(3)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
     if (!items.empty()) {
         if (L.persistent) {
             const int occ = bp_max_active_blocks(L);
