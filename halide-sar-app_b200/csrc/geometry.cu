@@ -1,6 +1,7 @@
 // geometry.cu -- f64 geometry of the pixel tiles, ahead of the FP32 loop.
 //
-// tile_setup_kernel (one CTA per (job, tile)):
+// tile_setup_kernel (one CTA per (job, tile)) forms the tile's geometry and
+// then its pulse records:
 //   rc    = centre of the bounding box of the tile's pixel positions
 //   wide  = k_c * (bounding-box half-diagonal) > kWideRad; then w0 = unit
 //           vector from rc to the mid-aperture antenna
@@ -9,7 +10,7 @@
 //   fin   = exp(+j k_c dr(pixel, P/2)) per pixel (backprojection.cpp:135),
 //           dr = |pos| - |r - pos| in f64, phase reduced in f64; wide tiles
 //           multiply in exp(-j w0 . k_c (r - rc)), also in f64
-// pulse_record_kernel (one thread per (tile, pulse)):
+// record of each pulse (make_record):
 //   w = pos - rc, R = |w|, dr_c = |pos| - R, t_c = (dr_c - lsa) / lsr,
 //   base = floor(t_c) - K, theta = k_c dr_c reduced to [-pi, pi),
 //   c0 = t_c - floor(t_c) + K - 1/2 - theta / (k_c lsr), and the series
@@ -45,6 +46,60 @@ __device__ __forceinline__ void pixel_pos(const DevJob &jb, int ix, int iy, doub
     }
 }
 
+// The record of pulse p for tile t (see the file comment); false when the
+// pulse has non-finite geometry (its window then stays zero).
+__device__ __forceinline__ bool make_record(const DevJob &jb, const TileInfo &t, double k_c, int p,
+                                            PulseRec &rec) {
+    const double4 g = jb.pulse[p];
+    const double wx = g.x - t.rc[0], wy = g.y - t.rc[1], wz = g.z - t.rc[2];
+    const double R2 = wx * wx + wy * wy + wz * wz;
+    const double iR = rsqrt(R2);  // 1/R and R from one reciprocal square root
+    const double R = R2 * iR;
+    const double drc = g.w - R;
+    double tc = (drc - jb.lsa) * jb.inv_lsr;
+    tc = fmin(fmax(tc, -1.0e8), 1.0e8);
+    const double fl = floor(tc);
+    if (isfinite(R) && R > 0.0 && isfinite(tc)) {
+        double th = drc * (k_c * kInv2Pi);
+        th = th - rint(th);
+        const double theta = kTwoPi * th;  // in [-pi, pi]
+        const float gm = (float)(t.rho * 0.5 * iR);                    // max |g| = rho / (2R)
+        const float kcf = (float)k_c;
+        // truncation of the series after 2, 3, 4 terms: C_n y^n |h| with
+        // y <= gm and |h| <= k_c rho (rad)
+        const float rk = t.rho * kcf;
+        const float e2 = 2.0f * rk * gm * gm;
+        const float e3 = 5.0f * rk * gm * gm * gm;
+        const float e4 = 14.0f * rk * gm * gm * gm * gm;
+        int order = (e4 > kPhaseTol || gm > 5e-3f) ? 3 : e3 > kPhaseTol ? 2 : e2 > kPhaseTol ? 1 : 0;
+        const int base = (int)fl - t.K;
+        const double e = 0.5 * iR / k_c;
+        const double c0 = (tc - fl) + ((double)t.K - 0.5) - theta * (jb.inv_lsr / k_c);
+        if (t.wide) {
+            rec.a = make_float4((float)(wx * iR - (double)t.w0[0]), (float)(wy * iR - (double)t.w0[1]),
+                                (float)(wz * iR - (double)t.w0[2]), (float)e);
+            rec.b = make_float4((float)c0, (float)theta, (float)(k_c * R), __int_as_float(8 * base + order));
+        } else {
+            // theta folded into the linear term: sigma = kappa (w_hat . d + theta)
+            // + e theta^2 with kappa = 1 - 2 e theta, so that theta + s + e t =
+            // sigma + e' (sigma^2 - |d|^2) + (e - e')(-|d|^2), e' = e / kappa^2;
+            // the last term is below 4 pi gm^2 rad and is added from series
+            // order 1 on, which tiles with gm > 4e-4 always use
+            if (gm > 4e-4f) order = max(order, 1);
+            const double kap = 1.0 - 2.0 * e * theta;
+            rec.a = make_float4((float)(kap * wx * iR), (float)(kap * wy * iR), (float)(kap * wz * iR),
+                                (float)(e / (kap * kap)));
+            rec.b = make_float4((float)c0, (float)(kap * theta + e * theta * theta), (float)(k_c * R),
+                                __int_as_float(8 * base + order));
+        }
+        return true;
+    }
+    // no contribution: the staging leaves this pulse's window at zero
+    rec.a = make_float4(0.f, 0.f, 0.f, 0.f);
+    rec.b = make_float4((float)t.K - 0.5f, 0.f, 1.f, __int_as_float(kOrderInvalid));
+    return false;
+}
+
 
 // pixels per thread of the largest tile (2048 pixels, 256 threads)
 constexpr int kGeomPix = 8;
@@ -64,6 +119,7 @@ __global__ void __launch_bounds__(kThreadsGeom) tile_setup_kernel(const DevJob *
     __shared__ double sbox[kWarps][6];
     __shared__ float srho[kWarps];
     __shared__ int sflags[kWarps][2];
+    __shared__ TileInfo s_tile;
     const WorkItem wi = items[blockIdx.x];
     const DevJob &jb = jobs[wi.job];
     const int TX = jb.tile_x, TY = jb.tile_y;
@@ -211,69 +267,20 @@ __global__ void __launch_bounds__(kThreadsGeom) tile_setup_kernel(const DevJob *
             }
         }
         jb.tiles[wi.tile] = t;
+        s_tile = t;
         if (bad) atomicOr(&jb.sc->status, kStatusNonFinite);
     }
-}
-
-// blockIdx.x = work item, blockIdx.y * blockDim.x + threadIdx.x = pulse
-__global__ void __launch_bounds__(kThreadsGeom) pulse_record_kernel(const DevJob *__restrict__ jobs,
-                                                                    const WorkItem *__restrict__ items) {
-    const WorkItem wi = items[blockIdx.x];
-    const DevJob &jb = jobs[wi.job];
-    const int p = blockIdx.y * blockDim.x + threadIdx.x;
-    if (p >= jb.P) return;
-    const TileInfo t = jb.tiles[wi.tile];
-    const double k_c = jb.sc->k_c;
-    const double4 g = jb.pulse[p];
-    const double wx = g.x - t.rc[0], wy = g.y - t.rc[1], wz = g.z - t.rc[2];
-    const double R2 = wx * wx + wy * wy + wz * wz;
-    const double iR = rsqrt(R2);  // 1/R and R from one reciprocal square root
-    const double R = R2 * iR;
-    const double drc = g.w - R;
-    double tc = (drc - jb.lsa) * jb.inv_lsr;
-    tc = fmin(fmax(tc, -1.0e8), 1.0e8);
-    const double fl = floor(tc);
-    PulseRec rec;
-    if (isfinite(R) && R > 0.0 && isfinite(tc)) {
-        double th = drc * (k_c * kInv2Pi);
-        th = th - rint(th);
-        const double theta = kTwoPi * th;  // in [-pi, pi]
-        const float gm = (float)(t.rho * 0.5 * iR);                    // max |g| = rho / (2R)
-        const float kcf = (float)k_c;
-        // truncation of the series after 2, 3, 4 terms: C_n y^n |h| with
-        // y <= gm and |h| <= k_c rho (rad)
-        const float rk = t.rho * kcf;
-        const float e2 = 2.0f * rk * gm * gm;
-        const float e3 = 5.0f * rk * gm * gm * gm;
-        const float e4 = 14.0f * rk * gm * gm * gm * gm;
-        int order = (e4 > kPhaseTol || gm > 5e-3f) ? 3 : e3 > kPhaseTol ? 2 : e2 > kPhaseTol ? 1 : 0;
-        const int base = (int)fl - t.K;
-        const double e = 0.5 * iR / k_c;
-        const double c0 = (tc - fl) + ((double)t.K - 0.5) - theta * (jb.inv_lsr / k_c);
-        if (t.wide) {
-            rec.a = make_float4((float)(wx * iR - (double)t.w0[0]), (float)(wy * iR - (double)t.w0[1]),
-                                (float)(wz * iR - (double)t.w0[2]), (float)e);
-            rec.b = make_float4((float)c0, (float)theta, (float)(k_c * R), __int_as_float(8 * base + order));
-        } else {
-            // theta folded into the linear term: sigma = kappa (w_hat . d + theta)
-            // + e theta^2 with kappa = 1 - 2 e theta, so that theta + s + e t =
-            // sigma + e' (sigma^2 - |d|^2) + (e - e')(-|d|^2), e' = e / kappa^2;
-            // the last term is below 4 pi gm^2 rad and is added from series
-            // order 1 on, which tiles with gm > 4e-4 always use
-            if (gm > 4e-4f) order = max(order, 1);
-            const double kap = 1.0 - 2.0 * e * theta;
-            rec.a = make_float4((float)(kap * wx * iR), (float)(kap * wy * iR), (float)(kap * wz * iR),
-                                (float)(e / (kap * kap)));
-            rec.b = make_float4((float)c0, (float)(kap * theta + e * theta * theta), (float)(k_c * R),
-                                __int_as_float(8 * base + order));
-        }
-    } else {
-        // no contribution: the staging leaves this pulse's window at zero
-        rec.a = make_float4(0.f, 0.f, 0.f, 0.f);
-        rec.b = make_float4((float)t.K - 0.5f, 0.f, 1.f, __int_as_float(kOrderInvalid));
-        atomicOr(&jb.sc->status, kStatusNonFinite);
+    __syncthreads();
+    // ---- this tile's pulse records ----
+    const TileInfo t = s_tile;
+    bool bad_pulse = false;
+    PulseRec *recs = jb.recs + (size_t)wi.tile * jb.P;
+    for (int p = threadIdx.x; p < jb.P; p += kThreadsGeom) {
+        PulseRec rec;
+        bad_pulse |= !make_record(jb, t, k_c, p, rec);
+        recs[p] = rec;
     }
-    jb.recs[(size_t)wi.tile * jb.P + p] = rec;
+    if (__any_sync(0xffffffffu, bad_pulse) && lane == 0) atomicOr(&jb.sc->status, kStatusNonFinite);
 }
 
 }  // namespace
@@ -284,12 +291,5 @@ cudaError_t launch_tile_setup(const DevJob *d_jobs, const WorkItem *d_items, int
     return cudaGetLastError();
 }
 
-cudaError_t launch_pulse_records(const DevJob *d_jobs, const WorkItem *d_items, int nitems, int max_p,
-                                 cudaStream_t st) {
-    if (nitems <= 0) return cudaSuccess;
-    const dim3 grid(nitems, (max_p + kThreadsGeom - 1) / kThreadsGeom);
-    pulse_record_kernel<<<grid, kThreadsGeom, 0, st>>>(d_jobs, d_items);
-    return cudaGetLastError();
-}
 
 }  // namespace sarbp

@@ -41,8 +41,7 @@ cudaError_t launch_backproject_naive(const DevJob *d_jobs, int job, int nu, int 
 
 // geometry.cu
 cudaError_t launch_tile_setup(const DevJob *d_jobs, const WorkItem *d_items, int nitems, cudaStream_t st);
-cudaError_t launch_pulse_records(const DevJob *d_jobs, const WorkItem *d_items, int nitems, int max_p,
-                                 cudaStream_t st);
+
 
 // peaks.cu
 cudaError_t measure_peaks(int num_sms, cudaStream_t st, double *ffma_per_s, double *mufu_per_s);

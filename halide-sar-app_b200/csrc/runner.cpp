@@ -480,7 +480,6 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
             if (last > first) {
                 const int n = (int)(last - first);
                 e = launch_tile_setup(d_jobs, d_items + first, n, sg);
-                if (e == cudaSuccess) e = launch_pulse_records(d_jobs, d_items + first, n, jobs[0].npulses, sg);
                 // one CTA per tile: the block scheduler then starts the next
                 // slab's CTAs (other stream) as this slab's last tiles finish
                 BpLaunch Lg = L;
@@ -488,7 +487,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
                 Lg.grid = n;
                 if (e == cudaSuccess) e = launch_backproject(Lg, d_jobs, d_items + first, n, d_cnt + 64 * g, sg);
                 if (e != cudaSuccess) return cuda_fail(e, "slab launch");
-                dev_->launches += 3;
+                dev_->launches += 2;
             }
             if ((e = cudaEventRecord(slabs->done[g], sg)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
         }
@@ -498,13 +497,9 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         items.clear();  // formed above
     }
     if (!items.empty()) {
-        int max_p = 0;
-        for (int i = 0; i < njobs; ++i)
-            if (prec[i] != SARBP_PREC_NAIVE) max_p = std::max(max_p, jobs[i].npulses);
         e = launch_tile_setup(d_jobs, d_items, (int)items.size(), st);
-        if (e == cudaSuccess) e = launch_pulse_records(d_jobs, d_items, (int)items.size(), max_p, st);
         if (e != cudaSuccess) return cuda_fail(e, "tile geometry launch");
-        dev_->launches += 2;
+        dev_->launches += 1;
     }
     if (!slabbed && (e = rec(3)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
     if (!items.empty()) {

@@ -399,7 +399,7 @@ def test_kernels_are_launched(ctx, cfg1):
     before = ctx.launch_count()
     ctx.backprojection_cuda(d["phs"], d["k_r"].astype(np.float32), d["taylor"], d["N_fft"], d["delta_r"],
                             d["u"], d["v"], d["pos"].astype(np.float32), d["r"])
-    # set-up and range compression, then tile set-up, pulse records and
-    # backprojection per row slab: 512 x 512 in 32-row tiles is 16 tile rows,
-    # pipelined as 2 slabs of 8
-    assert ctx.launch_count() - before == 2 + 3 * 2
+    # set-up and range compression, then tile geometry (with the pulse
+    # records) and backprojection per row slab: 512 x 512 in 32-row tiles is
+    # 16 tile rows, pipelined as 2 slabs of 8
+    assert ctx.launch_count() - before == 2 + 2 * 2
