@@ -136,3 +136,25 @@ def test_halide_shim_matches_c_abi(ctx, afrl_input, afrl_reference):
     L.img_output_u8.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_void_p]
     assert L.img_output_u8(ctypes.addressof(dB.buf), DB_MIN, DB_MAX, ctypes.addressof(u8.buf)) == 0
     assert np.array_equal(u8.arr, ctx.img_output_u8(dB.arr, DB_MIN, DB_MAX))
+
+
+def test_row_blocks_on_gpu_reassemble_the_image(ctx, afrl_input, afrl_reference):
+    """The per-rank work of the distributed mode (sarbp_b200.distributed),
+    run block by block on this GPU: three uneven blocks of output rows, each
+    formed as its own job, reassemble the whole image.  Block edges that do
+    not fall on 32-row tile edges give tiles with other centres, so the
+    match is to rounding (relative L2 < 1e-5), and to the oracle within the
+    compat tolerance."""
+    from sarbp_b200.distributed import cuda_compute, output_row_blocks, pixel_rows
+    pd, R = afrl_input, afrl_reference
+    ip = R["ip"]
+    nu, nv = ip["nu"], ip["nv"]
+    compute = cuda_compute(ctx, pd["phs"], pd["k_r"], TAYLOR, R["n_fft"], R["dr"], ip["u"], pd["pos"])
+    r3 = ip["pixel_locs"].reshape(3, nv, nu)
+    out = np.empty((nv, nu), np.complex128)
+    for y0, y1 in output_row_blocks(nv, 3):
+        a, b = pixel_rows(nv, y0, y1)
+        out[y0:y1] = compute(ip["v"][a:b], np.ascontiguousarray(r3[:, a:b, :].reshape(3, -1)))
+    whole = compute(ip["v"], ip["pixel_locs"])
+    assert rel_l2(out, whole) < 1e-5
+    assert rel_l2(out, R["img"]) < 1e-4
