@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--njobs", type=int, default=96, help="batch96: number of jobs")
     ap.add_argument("--serve-rates", default="20,50,100,200,400", help="serve: arrival rates (req/s)")
     ap.add_argument("--serve-requests", type=int, default=2000, help="serve: requests per rate")
+    ap.add_argument("--serve-lanes", type=int, default=3, help="serve: concurrent batches")
+    ap.add_argument("--serve-batch-work", type=float, default=0.0,
+                    help="serve: pixel*pulses per batch (0: library default)")
     return ap.parse_args()
 
 
@@ -570,7 +573,8 @@ def run_serve(args, rank, world, local_rank):
     nreq = args.serve_requests
     clocks = Clocks(gpu_uuid(torch, torch.device("cuda", local_rank))) if rank == 0 else None
     sweep = []
-    srv = sb.Server(ctx, hbm_cap_bytes=150e9, lanes=2, max_batch=32, precision=sb.PREC_PRECISE)
+    srv = sb.Server(ctx, hbm_cap_bytes=150e9, lanes=args.serve_lanes, max_batch=32,
+                    max_batch_work=args.serve_batch_work, precision=sb.PREC_PRECISE)
     try:
         # warm-up: every pool job once
         for k in range(len(pool)):
@@ -625,7 +629,8 @@ def run_serve(args, rank, world, local_rank):
         "dtype": "f32 (split-precision; f64 per-pulse set-up, PREC_PRECISE)",
         "data": "synthetic (seeded uneven jobs, Poisson arrivals)",
         "config": {"workload": "serve: %d requests per rate drawn from 96 uneven jobs (batch96 distribution), "
-                               "rates %s req/s, 2 lanes, batches <= 32, HBM budget 150 GB" % (nreq, args.serve_rates),
+                               "rates %s req/s, %d lanes, batches <= 32, HBM budget 150 GB"
+                               % (nreq, args.serve_rates, args.serve_lanes),
                    "parallelism": "replicas%d" % world, "latency": "submission to complex image in pinned host memory"},
         "sweep": sweep, "peak_device_bytes": peak, "clocks": clk, "synthesis_seconds": synth_s,
     }

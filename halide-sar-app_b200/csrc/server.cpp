@@ -99,7 +99,7 @@ struct sarbp_server {
     sarbp_opts launch{};
     size_t cap = 0;
     int max_batch = 32;
-    double max_work = 1.2e10;  // pixel*pulses per batch (bounds a batch's latency)
+    double max_work = 6e9;  // pixel*pulses per batch (bounds a batch's latency)
     cudaMemPool_t pool = nullptr;
     Clock::time_point t0 = Clock::now();
 
@@ -321,7 +321,7 @@ int sarbp_server_create(sarbp_ctx *ctx, const sarbp_opts *launch, double hbm_cap
     s->cap = (size_t)hbm_cap_bytes;
     s->max_batch = max_batch > 0 ? max_batch : 32;
     if (max_batch_work > 0) s->max_work = max_batch_work;
-    const int nl = lanes > 0 ? std::min(lanes, 8) : 2;
+    const int nl = lanes > 0 ? std::min(lanes, 8) : 3;
     cudaMemPoolProps props{};
     props.allocType = cudaMemAllocationTypePinned;
     props.location.type = cudaMemLocationTypeDevice;

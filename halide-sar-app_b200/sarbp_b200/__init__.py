@@ -265,7 +265,7 @@ class Server:
     (ERR_TIMEOUT while in flight); times(id) gives (submit, start, done)
     seconds on the server's clock."""
 
-    def __init__(self, ctx, hbm_cap_bytes=150e9, lanes=2, max_batch=32, max_batch_work=0.0,
+    def __init__(self, ctx, hbm_cap_bytes=150e9, lanes=3, max_batch=32, max_batch_work=0.0,
                  precision=None, **tune):
         o = _opts(precision, **tune)
         self._h = ctypes.c_void_p()

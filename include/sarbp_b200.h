@@ -201,8 +201,8 @@ int sarbp_plan_destroy(sarbp_plan *plan);
  * requests in arrival order while their device footprint (inputs, outputs,
  * and their batch's scratch) fits hbm_cap_bytes, uploads each phase history
  * once, and launches them as one batch on the first free of `lanes` streams
- * (default 2), at most max_batch requests (default 32) and max_batch_work
- * pixel*pulses (default 1.2e10, about 10 ms of work) per batch; batches of
+ * (default 3), at most max_batch requests (default 32) and max_batch_work
+ * pixel*pulses (default 6e9, about 5 ms of work) per batch; batches of
  * different lanes overlap on the device and complete in whichever order
  * they finish.  A request that cannot fit an idle
  * server fails with SARBP_ERR_ADMISSION.  `launch` (may be NULL) fixes the
