@@ -28,6 +28,38 @@ __device__ __forceinline__ uint8_t to_u8(double v, double lo, double hi) {
     return (uint8_t)n;
 }
 
+// u8 of one pixel.  The value is decided in f32 (|z|^2 rounded to f32, the
+// accurate logf), whose error is far below 1e-4 of a grey level for display
+// ranges of 0.1 dB and wider; a pixel whose f32 level lands within that
+// margin of an integer, of the clamps, or is not finite, is recomputed with
+// the reference's f64 formula.  Only the f64 path runs where dB itself is
+// written.
+struct U8Scale {
+    double m, lo, hi;
+    float inv_m2, k, q0, eps;  // q = k ln(|z|^2 / m^2) + q0 (grey levels)
+};
+
+__device__ __forceinline__ U8Scale u8_scale(double m, double lo, double hi) {
+    U8Scale u;
+    u.m = m;
+    u.lo = lo;
+    u.hi = hi;
+    const double g = 255.0 / (hi - lo);               // grey levels per dB
+    u.inv_m2 = (float)(1.0 / (m * m));
+    u.k = (float)(5.0 / kLn10F32 * g);                // 10 log10(a/m) = 5 ln(a^2/m^2) / ln 10
+    u.q0 = (float)(-lo * g);
+    u.eps = (float)(2e-5 * g + 1e-4);
+    return u;
+}
+
+__device__ __forceinline__ uint8_t u8_of(double2 z, const U8Scale &u) {
+    const double a2 = z.x * z.x + z.y * z.y;
+    const float q = fmaf(u.k, logf((float)a2 * u.inv_m2), u.q0);
+    const float f = q - floorf(q);
+    if (q > u.eps && q < 255.0f - u.eps && f > u.eps && f < 1.0f - u.eps) return (uint8_t)q;
+    return to_u8(10.0 * (log(sqrt(a2) / u.m) / kLn10F32), u.lo, u.hi);
+}
+
 __global__ void maxabs_kernel(const double2 *__restrict__ img, long long n,
                               unsigned long long *__restrict__ out) {
     double m = 0.0;
@@ -50,12 +82,17 @@ __global__ void db_u8_kernel(const double2 *__restrict__ img, long long n,
                              const unsigned long long *__restrict__ maxbits, double *__restrict__ dB,
                              uint8_t *__restrict__ u8, double lo, double hi) {
     const double m = __longlong_as_double((long long)*maxbits);
+    const U8Scale us = u8_scale(m, lo, hi);
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
         const double2 z = img[i];
+        if (!dB) {
+            u8[i] = u8_of(z, us);
+            continue;
+        }
         const double a = sqrt(z.x * z.x + z.y * z.y);
         const double d = 10.0 * (log(a / m) / kLn10F32);
-        if (dB) dB[i] = d;
+        dB[i] = d;
         if (u8) u8[i] = to_u8(d, lo, hi);
     }
 }
@@ -75,7 +112,7 @@ __global__ void batch_u8_kernel(const DevJob *__restrict__ jobs) {
     if (!jb.out_u8) return;
     const double m = __longlong_as_double((long long)jb.sc->maxabs);
     const long long n = (long long)jb.nu * jb.nv;
-    const double lo = jb.dB_min, hi = jb.dB_max;
+    const U8Scale us = u8_scale(m, jb.dB_min, jb.dB_max);
     const bool vec = ((reinterpret_cast<uintptr_t>(jb.out_u8) & 3) == 0);
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; 4 * q < n; q += stride) {
@@ -83,18 +120,10 @@ __global__ void batch_u8_kernel(const DevJob *__restrict__ jobs) {
         if (vec && i0 + 4 <= n) {
             uint32_t w = 0;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const double2 z = jb.out[i0 + k];
-                const double a = sqrt(z.x * z.x + z.y * z.y);
-                w |= (uint32_t)to_u8(10.0 * (log(a / m) / kLn10F32), lo, hi) << (8 * k);
-            }
+            for (int k = 0; k < 4; ++k) w |= (uint32_t)u8_of(jb.out[i0 + k], us) << (8 * k);
             *reinterpret_cast<uint32_t *>(jb.out_u8 + i0) = w;
         } else {
-            for (long long i = i0; i < n && i < i0 + 4; ++i) {
-                const double2 z = jb.out[i];
-                const double a = sqrt(z.x * z.x + z.y * z.y);
-                jb.out_u8[i] = to_u8(10.0 * (log(a / m) / kLn10F32), lo, hi);
-            }
+            for (long long i = i0; i < n && i < i0 + 4; ++i) jb.out_u8[i] = u8_of(jb.out[i], us);
         }
     }
 }

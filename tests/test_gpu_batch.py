@@ -106,3 +106,24 @@ def test_autotune_and_oracle(ctx, oracle, mixed_jobs):
                                      out_idx=idx)
         got = j.image().ravel()[idx]
         assert rel_l2(got, want) < 1e-4, (j.nu, j.P, j.S)
+
+
+@pytest.mark.parametrize("lo,hi", [(-40.0, 0.0), (-3.0, -1.0), (-80.0, 10.0)])
+def test_u8_stage_equals_reference_formula(ctx, oracle, mixed_jobs, lo, hi):
+    """The fused u8 stage (f32 decision with an f64 fallback near grey-level
+    edges) gives exactly the reference's u8 (img_output.cpp:18-51 through the
+    oracle) of the image it wrote, for wide and narrow display ranges."""
+    import torch
+    for j in mixed_jobs:
+        j.job.dB_min, j.job.dB_max = lo, hi
+    _zero(mixed_jobs)
+    ctx.run_jobs([j.job for j in mixed_jobs])
+    ctx.synchronize()
+    for j in mixed_jobs:
+        img = j.image()
+        want = oracle.img_output_u8(oracle.img_output_to_dB(img), lo, hi)
+        got = j.out_u8.cpu().numpy()
+        assert np.array_equal(got, want), (j.nu, int((got != want).sum()))
+    d = mixed_jobs[0].data.get("db", (-40.0, 0.0))
+    for j in mixed_jobs:
+        j.job.dB_min, j.job.dB_max = d
