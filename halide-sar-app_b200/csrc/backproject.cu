@@ -107,7 +107,7 @@ __device__ __forceinline__ void bulk_copy(void *dst, const void *src, uint32_t b
 // r = sqrt(R'(R' - 2h)) (near field), as its nonlinear part
 // N = (s Delta - |d|^2) / (R' + r), free of the cancellation in Delta - s.
 // Narrow tiles: the records carry kappa w_hat, e' and sigma0 = kappa theta +
-// e theta^2 (pulse-record kernel), so the phase theta + s + e t is
+// e theta^2 (tile geometry kernel), so the phase theta + s + e t is
 //     sigma = kappa w_hat . d + sigma0,   D = sigma + e' (sigma^2 - |d|^2)
 // (three FMAs for a planar tile), plus from MODE 1 on the small terms
 // (e - e')(-|d|^2) and the higher series terms, formed from

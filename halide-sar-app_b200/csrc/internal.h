@@ -48,7 +48,7 @@ struct __align__(16) TileInfo {
     int transposed;  // 1: consumer lanes run along y (square tiles; see tile set-up)
 };
 
-// Per-(tile, pulse) constants (pulse-record kernel -> backprojection):
+// Per-(tile, pulse) constants (tile geometry kernel -> backprojection):
 //   a = (w_hat.x, w_hat.y, w_hat.z, e = 1/(2 k_c R)); wide tiles: w_hat - w0
 //   b = (c0 - theta*inv_lsr/k_c, theta, k_c R, int bits: 8*base + series order)
 // series order 0..3 (see the backprojection kernel); kOrderInvalid marks a
