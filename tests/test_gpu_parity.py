@@ -394,6 +394,35 @@ def test_errors_are_codes(sb, ctx, cfg1):
     assert np.all(np.isfinite(img))
 
 
+def test_bad_pixels_and_sizes_are_codes(sb, ctx, cfg1):
+    """A non-finite pixel position is SARBP_ERR_GEOMETRY (one NaN in one
+    coordinate, and an infinity), empty image or pulse extents are
+    SARBP_ERR_INVALID; the context keeps working and gives the same image
+    as before."""
+    d = cfg1
+    pos32, k32 = d["pos"].astype(np.float32), d["k_r"].astype(np.float32)
+    good = ctx.backprojection_cuda(d["phs"], k32, d["taylor"], d["N_fft"], d["delta_r"], d["u"], d["v"],
+                                   pos32, d["r"])
+    for coord, val in ((2, np.nan), (0, np.inf)):
+        r = d["r"].copy()
+        r[coord, 777] = val
+        with pytest.raises(sb.SarbpError) as e:
+            ctx.backprojection_cuda(d["phs"], k32, d["taylor"], d["N_fft"], d["delta_r"], d["u"], d["v"],
+                                    pos32, r)
+        assert e.value.code == sb._lib.ERR_GEOMETRY
+    with pytest.raises(sb.SarbpError) as e:
+        ctx.backprojection_cuda(d["phs"], k32, d["taylor"], d["N_fft"], d["delta_r"], d["u"][:0], d["v"],
+                                pos32, d["r"][:, :0])
+    assert e.value.code == sb._lib.ERR_INVALID
+    with pytest.raises(sb.SarbpError) as e:
+        ctx.backprojection_cuda(d["phs"][:0], k32, d["taylor"], d["N_fft"], d["delta_r"], d["u"], d["v"],
+                                pos32[:0], d["r"])
+    assert e.value.code == sb._lib.ERR_INVALID
+    again = ctx.backprojection_cuda(d["phs"], k32, d["taylor"], d["N_fft"], d["delta_r"], d["u"], d["v"],
+                                    pos32, d["r"])
+    assert np.array_equal(again, good)
+
+
 def test_kernels_are_launched(ctx, cfg1):
     d = cfg1
     before = ctx.launch_count()
