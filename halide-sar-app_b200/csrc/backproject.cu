@@ -122,107 +122,117 @@ __device__ __forceinline__ void bulk_copy(void *dst, const void *src, uint32_t b
 // instruction, the same rounding as two scalar operations), so every
 // per-pixel FP32 step up to the range bin costs half an issue slot; the
 // window loads, the interpolation and the sine/cosine stay per pixel.  Each
-// record is staged as four float4 of broadcast pairs (see expand_records).
+// record is staged as four float4 of broadcast pairs (see stage_chunk).
 // The images are the same bit for bit as with scalar arithmetic.
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
+// One pulse (record rec, window at byte offset poff) for a consumer's pixel
+// pairs.  The sine and cosine are written straight into the pair registers
+// that the accumulation's f32x2 FMAs read.
 template <int MODE, bool PLANAR, bool WIDE, int NP>
-__device__ __forceinline__ void accumulate(int nc, const float4 *__restrict__ rec2, uint32_t poff,
-                                           uint32_t pstride, float2 ILK, float hi_clamp,
+__device__ __forceinline__ void pulse_step(const float4 *__restrict__ rec, uint32_t poff, float2 ILK, float2 CL,
                                            const float2 (&dx)[NP], const float2 (&dy)[NP],
                                            const float2 (&dz)[NP], const float2 (&nd2)[NP],
                                            const float2 (&s0)[NP], float2 (&ar)[NP], float2 (&ai)[NP]) {
-    const float2 M2 = f2(kMagic, kMagic), NM2 = f2(-kMagic, -kMagic), NEG1 = f2(-1.0f, -1.0f);
-#pragma unroll 2
-    for (int i = 0; i < nc; ++i, poff += pstride) {
-        const float4 q0 = rec2[4 * i];      // ax ax ay ay   (narrow: kappa w_hat; wide: w_hat - w0)
-        const float4 q1 = rec2[4 * i + 1];  // az az e  e    (narrow: e')
-        const float4 q2 = rec2[4 * i + 2];  // c0 c0 b  b    (narrow: sigma0; wide: theta)
-        const float2 AX = f2(q0.x, q0.y), AY = f2(q0.z, q0.w), AZ = f2(q1.x, q1.y);
-        const float2 E = f2(q1.z, q1.w), C0 = f2(q2.x, q2.y), B = f2(q2.z, q2.w);
-        float Rp = 0.0f;
-        if constexpr (MODE == 3) Rp = rec2[4 * i + 3].x;
-        const float ee = q1.z * q1.z;
-        const float2 EE = f2(ee, ee);
-        const float de = -4.0f * ee * q2.z;  // e - e' (narrow tiles)
-        const float2 DE = f2(de, de);
+    const float2 M2 = f2(kMagic), NEG1 = f2(-1.0f);
+    const float4 q0 = rec[0];  // ax ax ay ay   (narrow: kappa w_hat; wide: w_hat - w0)
+    const float4 q1 = rec[1];  // az az e  e    (narrow: e')
+    const float4 q2 = rec[2];  // c0 c0 b  b    (narrow: sigma0; wide: theta)
+    const float2 AX = f2(q0.x, q0.y), AY = f2(q0.z, q0.w), AZ = f2(q1.x, q1.y);
+    const float2 E = f2(q1.z, q1.w), C0 = f2(q2.x, q2.y), B = f2(q2.z, q2.w);
+    float Rp = 0.0f;
+    if constexpr (MODE == 3) Rp = rec[3].x;
+    const float ee = q1.z * q1.z;
+    const float2 EE = f2(ee);
+    const float de = -4.0f * ee * q2.z;  // e - e' (narrow tiles)
+    const float2 DE = f2(de);
 #pragma unroll
-        for (int j = 0; j < NP; ++j) {
-            float2 D, s;  // phase argument; s = w_hat . d (approximate for narrow tiles)
-            if constexpr (!WIDE) {
-                float2 sg = __ffma2_rn(AX, dx[j], B);
-                sg = __ffma2_rn(AY, dy[j], sg);
-                if constexpr (!PLANAR) sg = __ffma2_rn(AZ, dz[j], sg);
-                D = __ffma2_rn(E, __ffma2_rn(sg, sg, nd2[j]), sg);
-                s = __ffma2_rn(B, NEG1, sg);
-                if constexpr (MODE >= 1) D = __ffma2_rn(DE, nd2[j], D);
-            } else {
-                float2 sd = __fmul2_rn(AX, dx[j]);
-                sd = __ffma2_rn(AY, dy[j], sd);
-                if constexpr (!PLANAR) sd = __ffma2_rn(AZ, dz[j], sd);
-                s = __fadd2_rn(s0[j], sd);
-                D = __fadd2_rn(__ffma2_rn(E, __ffma2_rn(s, s, nd2[j]), sd), B);
-            }
-            if constexpr (MODE == 1) {
-                D = __ffma2_rn(__fmul2_rn(__fadd2_rn(EE, EE), s), __ffma2_rn(s, s, nd2[j]), D);
-            } else if constexpr (MODE == 2) {
-                const float2 h = __ffma2_rn(E, nd2[j], s);
-                const float2 q = __ffma2_rn(__fmul2_rn(f2(5.0f, 5.0f), E), h, f2(2.0f, 2.0f));
-                const float2 h3 = __fmul2_rn(__fmul2_rn(h, h), h);
-                D = __ffma2_rn(EE, __ffma2_rn(h3, q, __fmul2_rn(nd2[j], __fadd2_rn(h, s))), D);
-            } else if constexpr (MODE == 3) {
-                float n[2];
-#pragma unroll
-                for (int l = 0; l < 2; ++l) {
-                    const float sl = l ? s.y : s.x, nl = l ? nd2[j].y : nd2[j].x, el = q1.z;
-                    const float h = fmaf(el, nl, sl);
-                    const float q = fmaxf(fmaf(-2.0f, h, Rp), 0.0f);
-                    const float den = Rp + sqrtf(Rp * q);
-                    const float Dn = __fdividef(2.0f * Rp * h, den);
-                    // exact nonlinear part less the two-term one
-                    n[l] = __fdividef(fmaf(sl, Dn, nl), den) - el * fmaf(sl, sl, nl);
-                }
-                D = __fadd2_rn(D, f2(n[0], n[1]));
-            }
-            const float2 Di = WIDE ? __fadd2_rn(s0[j], D) : D;  // range-bin argument
-            float2 tl = __ffma2_rn(Di, ILK, C0);
-            if constexpr (MODE >= 2) {
-                tl.x = fminf(fmaxf(tl.x, 0.0f), hi_clamp);
-                tl.y = fminf(fmaxf(tl.y, 0.0f), hi_clamp);
-            }
-            const float2 f = __fadd2_rn(tl, M2);
-            const float2 w = __ffma2_rn(__fadd2_rn(f, NM2), NEG1, tl);  // tl - floor(tl)
-            float4 m0, m1;
-            const uint32_t o0 = (__float_as_uint(f.x) << 4) + poff;  // shared-window addresses
-            const uint32_t o1 = (__float_as_uint(f.y) << 4) + poff;
-            asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
-                         : "=f"(m0.x), "=f"(m0.y), "=f"(m0.z), "=f"(m0.w)
-                         : "r"(o0));
-            asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
-                         : "=f"(m1.x), "=f"(m1.y), "=f"(m1.z), "=f"(m1.w)
-                         : "r"(o1));
-            const float vr0 = fmaf(w.x, m0.z, m0.x), vi0 = fmaf(w.x, m0.w, m0.y);
-            const float vr1 = fmaf(w.y, m1.z, m1.x), vi1 = fmaf(w.y, m1.w, m1.y);
-            float sn0, cs0, sn1, cs1;
-            __sincosf(D.x, &sn0, &cs0);
-            __sincosf(D.y, &sn1, &cs1);
-            const float2 VR = f2(vr0, vr1), VI = f2(vi0, vi1), SN = f2(sn0, sn1), CS = f2(cs0, cs1);
-            ar[j] = __ffma2_rn(VR, CS, __ffma2_rn(VI, SN, ar[j]));
-            float2 t = __ffma2_rn(VI, CS, ai[j]);
-            t.x = fmaf(-vr0, sn0, t.x);
-            t.y = fmaf(-vr1, sn1, t.y);
-            ai[j] = t;
+    for (int j = 0; j < NP; ++j) {
+        float2 D, s;  // phase argument; s = w_hat . d (approximate for narrow tiles)
+        if constexpr (!WIDE) {
+            float2 sg = __ffma2_rn(AX, dx[j], B);
+            sg = __ffma2_rn(AY, dy[j], sg);
+            if constexpr (!PLANAR) sg = __ffma2_rn(AZ, dz[j], sg);
+            D = __ffma2_rn(E, __ffma2_rn(sg, sg, nd2[j]), sg);
+            s = __ffma2_rn(B, NEG1, sg);
+            if constexpr (MODE >= 1) D = __ffma2_rn(DE, nd2[j], D);
+        } else {
+            float2 sd = __fmul2_rn(AX, dx[j]);
+            sd = __ffma2_rn(AY, dy[j], sd);
+            if constexpr (!PLANAR) sd = __ffma2_rn(AZ, dz[j], sd);
+            s = __fadd2_rn(s0[j], sd);
+            D = __fadd2_rn(__ffma2_rn(E, __ffma2_rn(s, s, nd2[j]), sd), B);
         }
+        if constexpr (MODE == 1) {
+            D = __ffma2_rn(__fmul2_rn(__fadd2_rn(EE, EE), s), __ffma2_rn(s, s, nd2[j]), D);
+        } else if constexpr (MODE == 2) {
+            const float2 h = __ffma2_rn(E, nd2[j], s);
+            const float2 q = __ffma2_rn(__fmul2_rn(f2(5.0f), E), h, f2(2.0f));
+            const float2 h3 = __fmul2_rn(__fmul2_rn(h, h), h);
+            D = __ffma2_rn(EE, __ffma2_rn(h3, q, __fmul2_rn(nd2[j], __fadd2_rn(h, s))), D);
+        } else if constexpr (MODE == 3) {
+            float n[2];
+#pragma unroll
+            for (int l = 0; l < 2; ++l) {
+                const float sl = l ? s.y : s.x, nl = l ? nd2[j].y : nd2[j].x, el = q1.z;
+                const float h = fmaf(el, nl, sl);
+                const float q = fmaxf(fmaf(-2.0f, h, Rp), 0.0f);
+                const float den = Rp + sqrtf(Rp * q);
+                const float Dn = __fdividef(2.0f * Rp * h, den);
+                // exact nonlinear part less the two-term one
+                n[l] = __fdividef(fmaf(sl, Dn, nl), den) - el * fmaf(sl, sl, nl);
+            }
+            D = __fadd2_rn(D, f2(n[0], n[1]));
+        }
+        const float2 Di = WIDE ? __fadd2_rn(s0[j], D) : D;  // range-bin argument
+        float2 tl = __ffma2_rn(Di, ILK, C0);
+        if constexpr (MODE >= 2) {
+            tl.x = fminf(fmaxf(tl.x, CL.x), CL.y);
+            tl.y = fminf(fmaxf(tl.y, CL.x), CL.y);
+        }
+        const float2 f = __fadd2_rn(tl, M2);
+        const float2 w = __ffma2_rn(__fadd2_rn(f, f2(-kMagic)), NEG1, tl);  // tl - rint(tl)
+        float4 m0, m1;
+        const uint32_t o0 = (__float_as_uint(f.x) << 4) + poff;  // shared-window addresses
+        const uint32_t o1 = (__float_as_uint(f.y) << 4) + poff;
+        asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                     : "=f"(m0.x), "=f"(m0.y), "=f"(m0.z), "=f"(m0.w)
+                     : "r"(o0));
+        asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                     : "=f"(m1.x), "=f"(m1.y), "=f"(m1.z), "=f"(m1.w)
+                     : "r"(o1));
+        const float vr0 = fmaf(w.x, m0.z, m0.x), vi0 = fmaf(w.x, m0.w, m0.y);
+        const float vr1 = fmaf(w.y, m1.z, m1.x), vi1 = fmaf(w.y, m1.w, m1.y);
+        float2 SN, CS;
+        __sincosf(D.x, &SN.x, &CS.x);
+        __sincosf(D.y, &SN.y, &CS.y);
+        const float2 VR = f2(vr0, vr1), VI = f2(vi0, vi1);
+        ar[j] = __ffma2_rn(VR, CS, __ffma2_rn(VI, SN, ar[j]));
+        ai[j] = __ffma2_rn(f2(-vr0, -vr1), SN, __ffma2_rn(VI, CS, ai[j]));  // negation folds into the FMA
     }
+}
+
+// Inner loop over the nc pulses of a chunk (records rec2, windows from byte
+// offset poff, pstride bytes apart); CL clamps the bin argument (modes 2, 3).
+template <int MODE, bool PLANAR, bool WIDE, int NP>
+__device__ __forceinline__ void accumulate(int nc, const float4 *__restrict__ rec2, uint32_t poff,
+                                           uint32_t pstride, float2 ILK, float2 CL,
+                                           const float2 (&dx)[NP], const float2 (&dy)[NP],
+                                           const float2 (&dz)[NP], const float2 (&nd2)[NP],
+                                           const float2 (&s0)[NP], float2 (&ar)[NP], float2 (&ai)[NP]) {
+#pragma unroll 2
+    for (int i = 0; i < nc; ++i, poff += pstride)
+        pulse_step<MODE, PLANAR, WIDE, NP>(rec2 + 4 * i, poff, ILK, CL, dx, dy, dz, nd2, s0, ar, ai);
 }
 
 template <bool WIDE, int NP>
 __device__ __forceinline__ void accumulate_mode(int mode, bool planar, int nc, const float4 *rec2,
-                                                uint32_t poff, uint32_t pstride, float2 ILK, float hi,
+                                                uint32_t poff, uint32_t pstride, float2 ILK, float2 CL,
                                                 const float2 (&dx)[NP], const float2 (&dy)[NP],
                                                 const float2 (&dz)[NP], const float2 (&nd2)[NP],
                                                 const float2 (&s0)[NP], float2 (&ar)[NP], float2 (&ai)[NP]) {
-#define SARBP_ACC(M, PL) accumulate<M, PL, WIDE, NP>(nc, rec2, poff, pstride, ILK, hi, dx, dy, dz, nd2, s0, ar, ai)
+#define SARBP_ACC(M, PL) accumulate<M, PL, WIDE, NP>(nc, rec2, poff, pstride, ILK, CL, dx, dy, dz, nd2, s0, ar, ai)
     if (mode == 0) {
         if (planar) SARBP_ACC(0, true);
         else SARBP_ACC(0, false);
@@ -453,7 +463,7 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
         } else {
             const float ilk = (float)(jb.inv_lsr / k_c);  // range bins per radian of Delta
             const float2 ILK = make_float2(ilk, ilk);
-            const float hi = (float)(sh.W - 1) - 0.5f;
+            const float2 CL = f2(0.0f, (float)(sh.W - 1) - 0.5f);  // bin-argument clamp (modes 2, 3)
             const uint32_t pstride = (uint32_t)sh.W * 16u;
             for (int c = 0; c < sh.nchunks; ++c) {
                 const int b = c & 1;
@@ -463,10 +473,10 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
                 const int nc = min(sh.C, P - p0);
                 const float4 *rec2 = sm.rec2 + (size_t)b * 4 * cmax;
                 if (ti.wide)
-                    accumulate_mode<true, NP>(sm.s_mode[b], ti.planar != 0, nc, rec2, poff, pstride, ILK, hi,
+                    accumulate_mode<true, NP>(sm.s_mode[b], ti.planar != 0, nc, rec2, poff, pstride, ILK, CL,
                                               dxp, dyp, dzp, nd2p, s0p, arp, aip);
                 else
-                    accumulate_mode<false, NP>(sm.s_mode[b], ti.planar != 0, nc, rec2, poff, pstride, ILK, hi,
+                    accumulate_mode<false, NP>(sm.s_mode[b], ti.planar != 0, nc, rec2, poff, pstride, ILK, CL,
                                                dxp, dyp, dzp, nd2p, s0p, arp, aip);
                 bar_arrive(kBarEmpty0 + b);
             }

@@ -46,10 +46,16 @@ __device__ __forceinline__ void pixel_pos(const DevJob &jb, int ix, int iy, doub
     }
 }
 
+// Per-job constants of the records: k_c, 1/(2 k_c), 1/(k_c lsr).
+struct RecConst {
+    double k_c, half_inv_kc, ilk;
+};
+
 // The record of pulse p for tile t (see the file comment); false when the
 // pulse has non-finite geometry (its window then stays zero).
-__device__ __forceinline__ bool make_record(const DevJob &jb, const TileInfo &t, double k_c, int p,
+__device__ __forceinline__ bool make_record(const DevJob &jb, const TileInfo &t, const RecConst &cst, int p,
                                             PulseRec &rec) {
+    const double k_c = cst.k_c;
     const double4 g = jb.pulse[p];
     const double wx = g.x - t.rc[0], wy = g.y - t.rc[1], wz = g.z - t.rc[2];
     const double R2 = wx * wx + wy * wy + wz * wz;
@@ -73,8 +79,8 @@ __device__ __forceinline__ bool make_record(const DevJob &jb, const TileInfo &t,
         const float e4 = 14.0f * rk * gm * gm * gm * gm;
         int order = (e4 > kPhaseTol || gm > 5e-3f) ? 3 : e3 > kPhaseTol ? 2 : e2 > kPhaseTol ? 1 : 0;
         const int base = (int)fl - t.K;
-        const double e = 0.5 * iR / k_c;
-        const double c0 = (tc - fl) + ((double)t.K - 0.5) - theta * (jb.inv_lsr / k_c);
+        const double e = iR * cst.half_inv_kc;
+        const double c0 = (tc - fl) + ((double)t.K - 0.5) - theta * cst.ilk;
         if (t.wide) {
             rec.a = make_float4((float)(wx * iR - (double)t.w0[0]), (float)(wy * iR - (double)t.w0[1]),
                                 (float)(wz * iR - (double)t.w0[2]), (float)e);
@@ -86,9 +92,12 @@ __device__ __forceinline__ bool make_record(const DevJob &jb, const TileInfo &t,
             // the last term is below 4 pi gm^2 rad and is added from series
             // order 1 on, which tiles with gm > 4e-4 always use
             if (gm > 4e-4f) order = max(order, 1);
-            const double kap = 1.0 - 2.0 * e * theta;
+            const double x = 2.0 * e * theta, kap = 1.0 - x;
+            // 1 / kappa^2 = 1 + 2x + 3x^2 + 4x^3 + ... (|x| <= pi / (k_c R)); the
+            // series through x^3 is exact to f64 rounding for |x| < 1e-3
+            const double ik2 = fabs(x) < 1e-3 ? fma(x, fma(x, fma(x, 4.0, 3.0), 2.0), 1.0) : 1.0 / (kap * kap);
             rec.a = make_float4((float)(kap * wx * iR), (float)(kap * wy * iR), (float)(kap * wz * iR),
-                                (float)(e / (kap * kap)));
+                                (float)(e * ik2));
             rec.b = make_float4((float)c0, (float)(kap * theta + e * theta * theta), (float)(k_c * R),
                                 __int_as_float(8 * base + order));
         }
@@ -101,8 +110,6 @@ __device__ __forceinline__ bool make_record(const DevJob &jb, const TileInfo &t,
 }
 
 
-// pixels per thread of the largest tile (2048 pixels, 256 threads)
-constexpr int kGeomPix = 8;
 
 __device__ __forceinline__ double warp_min_d(double v) {
     for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -113,8 +120,11 @@ __device__ __forceinline__ double warp_max_d(double v) {
     return v;
 }
 
-__global__ void __launch_bounds__(kThreadsGeom) tile_setup_kernel(const DevJob *__restrict__ jobs,
-                                                                  const WorkItem *__restrict__ items) {
+// GP: pixels per thread (tile pixels / 256: 2, 4 or 8), kept in registers
+// between the two passes; up to 4 the registers fit three CTAs per SM.
+template <int GP>
+__global__ void __launch_bounds__(kThreadsGeom, GP <= 4 ? 3 : 2)
+    tile_setup_kernel(const DevJob *__restrict__ jobs, const WorkItem *__restrict__ items) {
     constexpr int kWarps = kThreadsGeom / 32;
     __shared__ double sbox[kWarps][6];
     __shared__ float srho[kWarps];
@@ -127,12 +137,12 @@ __global__ void __launch_bounds__(kThreadsGeom) tile_setup_kernel(const DevJob *
     const int tx0 = (wi.tile % jb.tiles_x) * TX, ty0 = (wi.tile / jb.tiles_x) * TY;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // this thread's pixels, kept in registers for both passes
-    double px[kGeomPix], py[kGeomPix], pz[kGeomPix];
+    double px[GP], py[GP], pz[GP];
     unsigned live = 0u;  // bit k: pixel k is inside the image and finite
     double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
     int bad = 0;
 #pragma unroll
-    for (int k = 0; k < kGeomPix; ++k) {
+    for (int k = 0; k < GP; ++k) {
         px[k] = py[k] = pz[k] = 0.0;
         const int idx = threadIdx.x + k * kThreadsGeom;
         if (idx >= TX * TY) continue;
@@ -193,7 +203,7 @@ __global__ void __launch_bounds__(kThreadsGeom) tile_setup_kernel(const DevJob *
     float rho = 0.0f;
     int planar = 1;
 #pragma unroll
-    for (int k = 0; k < kGeomPix; ++k) {
+    for (int k = 0; k < GP; ++k) {
         const int idx = threadIdx.x + k * kThreadsGeom;
         if (idx >= TX * TY) continue;
         const int ix = tx0 + (idx & (TX - 1)), iy = ty0 + (idx >> lx);
@@ -275,9 +285,13 @@ __global__ void __launch_bounds__(kThreadsGeom) tile_setup_kernel(const DevJob *
     const TileInfo t = s_tile;
     bool bad_pulse = false;
     PulseRec *recs = jb.recs + (size_t)wi.tile * jb.P;
+    RecConst rk;
+    rk.k_c = k_c;
+    rk.half_inv_kc = 0.5 / k_c;
+    rk.ilk = jb.inv_lsr / k_c;
     for (int p = threadIdx.x; p < jb.P; p += kThreadsGeom) {
         PulseRec rec;
-        bad_pulse |= !make_record(jb, t, k_c, p, rec);
+        bad_pulse |= !make_record(jb, t, rk, p, rec);
         recs[p] = rec;
     }
     if (__any_sync(0xffffffffu, bad_pulse) && lane == 0) atomicOr(&jb.sc->status, kStatusNonFinite);
@@ -285,9 +299,16 @@ __global__ void __launch_bounds__(kThreadsGeom) tile_setup_kernel(const DevJob *
 
 }  // namespace
 
-cudaError_t launch_tile_setup(const DevJob *d_jobs, const WorkItem *d_items, int nitems, cudaStream_t st) {
+cudaError_t launch_tile_setup(const DevJob *d_jobs, const WorkItem *d_items, int nitems, int tile_pixels,
+                              cudaStream_t st) {
     if (nitems <= 0) return cudaSuccess;
-    tile_setup_kernel<<<nitems, kThreadsGeom, 0, st>>>(d_jobs, d_items);
+    if (tile_pixels < 1 || tile_pixels > 8 * kThreadsGeom) return cudaErrorInvalidValue;
+    if (tile_pixels <= 2 * kThreadsGeom)
+        tile_setup_kernel<2><<<nitems, kThreadsGeom, 0, st>>>(d_jobs, d_items);
+    else if (tile_pixels <= 4 * kThreadsGeom)
+        tile_setup_kernel<4><<<nitems, kThreadsGeom, 0, st>>>(d_jobs, d_items);
+    else
+        tile_setup_kernel<8><<<nitems, kThreadsGeom, 0, st>>>(d_jobs, d_items);
     return cudaGetLastError();
 }
 

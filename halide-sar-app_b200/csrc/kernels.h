@@ -40,7 +40,8 @@ cudaError_t launch_backproject(const BpLaunch &L, const DevJob *d_jobs, const Wo
 cudaError_t launch_backproject_naive(const DevJob *d_jobs, int job, int nu, int nv, cudaStream_t st);
 
 // geometry.cu
-cudaError_t launch_tile_setup(const DevJob *d_jobs, const WorkItem *d_items, int nitems, cudaStream_t st);
+cudaError_t launch_tile_setup(const DevJob *d_jobs, const WorkItem *d_items, int nitems, int tile_pixels,
+                              cudaStream_t st);
 
 
 // peaks.cu

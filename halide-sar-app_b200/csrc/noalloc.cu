@@ -230,7 +230,7 @@ extern "C" int sarbp_backprojection_noalloc(const sarbp_job *job, void *cuda_str
     if (e != cudaSuccess) return cuda_fail(e, "no-alloc set-up launches");
     launch_prep(d_job, 1, st);
     e = launch_range_compress(logN, d_job, d_rows, j.npulses, 1, d_tw, st);
-    if (e == cudaSuccess) e = launch_tile_setup(d_job, d_items, (int)ntiles, st);
+    if (e == cudaSuccess) e = launch_tile_setup(d_job, d_items, (int)ntiles, L0.tile_x * L0.tile_y, st);
     if (e != cudaSuccess) return cuda_fail(e, "no-alloc range compression / geometry launch");
     BpLaunch L = L0;
     const int occ = bp_max_active_blocks(L);

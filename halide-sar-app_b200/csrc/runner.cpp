@@ -479,7 +479,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
                 return cuda_fail(e, "cudaStreamWaitEvent");
             if (last > first) {
                 const int n = (int)(last - first);
-                e = launch_tile_setup(d_jobs, d_items + first, n, sg);
+                e = launch_tile_setup(d_jobs, d_items + first, n, L.tile_x * L.tile_y, sg);
                 // one CTA per tile: the block scheduler then starts the next
                 // slab's CTAs (other stream) as this slab's last tiles finish
                 BpLaunch Lg = L;
@@ -497,7 +497,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         items.clear();  // formed above
     }
     if (!items.empty()) {
-        e = launch_tile_setup(d_jobs, d_items, (int)items.size(), st);
+        e = launch_tile_setup(d_jobs, d_items, (int)items.size(), L.tile_x * L.tile_y, st);
         if (e != cudaSuccess) return cuda_fail(e, "tile geometry launch");
         dev_->launches += 1;
     }
