@@ -565,6 +565,7 @@ def run_batch(args, rank, world, local_rank):
                          % (sum(j.device_bytes() for j in jobs) / 1e9)},
         "gpu_launches": int(launches),
         "autotuned": {"tile": list(tune["tile"]), "pulse_chunk": tune["pulse_chunk"],
+                      "stage_cap": tune.get("stage_cap", 0),
                       "min_blocks": tune["min_blocks"], "best_ms": tune_ms, "seconds": tune_s},
         "compare": {
             "graph_replay": g(ms_graph, args.steps),

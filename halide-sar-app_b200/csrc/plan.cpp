@@ -155,7 +155,7 @@ int sarbp_autotune(sarbp_ctx *ctx, const sarbp_job *jobs, int njobs, sarbp_opts 
         inout->precision = prec;
         return SARBP_OK;
     }
-    static const Candidate kCands[] = {{32, 32, 3}, {32, 16, 3}, {64, 16, 3}, {16, 32, 3}, {32, 8, 3},
+    static const Candidate kCands[] = {{32, 32, 3}, {32, 16, 3}, {64, 16, 3}, {16, 32, 3},
                                        {32, 32, 2}, {32, 64, 2}, {64, 32, 2}, {16, 64, 2}};
     static const int kChunks[] = {32, 64, 128};
     DeviceInfo &d = ctx->dev;
@@ -185,6 +185,11 @@ int sarbp_autotune(sarbp_ctx *ctx, const sarbp_job *jobs, int njobs, sarbp_opts 
             o.tile_y = c.ty;
             o.min_blocks = c.minb;
             o.pulse_chunk = chunk;
+            // at 2 CTAs/SM the staging buffer takes the shared memory the
+            // third CTA would have had (longer chunks for wide windows):
+            // half of 228 KB less 2 KB of reserve and the chunk's records
+            // (32 + 128 B per pulse), in 32-byte pairs of halves
+            o.stage_cap = c.minb == 2 ? (int)(((228 << 10) / 2 - 2048 - 160 * chunk) / 32) & ~1 : 0;
             float ms = 0.0f;
             rc = time_once(o, &ms);
             if (rc) break;

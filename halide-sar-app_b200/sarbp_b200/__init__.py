@@ -251,7 +251,8 @@ class Context:
         o = _opts(precision)
         ms = ctypes.c_float()
         check(lib().sarbp_autotune(self._h, arr, len(jobs), ctypes.byref(o), ctypes.byref(ms)))
-        tune = dict(tile=(o.tile_x, o.tile_y), pulse_chunk=o.pulse_chunk, min_blocks=o.min_blocks)
+        tune = dict(tile=(o.tile_x, o.tile_y), pulse_chunk=o.pulse_chunk, min_blocks=o.min_blocks,
+                    stage_cap=o.stage_cap)
         return tune, ms.value
 
     def plan(self, jobs, precision=None, **tune):

@@ -232,10 +232,11 @@ int sarbp_server_destroy(sarbp_server *server);
 
 /*
  * Launch-shape autotuner: runs the batch with each candidate pixel tile
- * (32x32, 32x16, 64x16, 16x32, 32x8 at 3 CTAs/SM; 32x32, 32x64, 64x32,
- * 16x64 at 2) and pulse-chunk depth (32, 64, 128), times set-up through
- * backprojection with CUDA events, re-times the three fastest, and writes
- * the fastest tile_x, tile_y, min_blocks and pulse_chunk into *inout (other
+ * (32x32, 32x16, 64x16, 16x32 at 3 CTAs/SM; 32x32, 32x64, 64x32, 16x64 at
+ * 2, with the staging buffer grown into the third CTA's shared memory) and
+ * pulse-chunk depth (32, 64, 128), times set-up through backprojection
+ * with CUDA events, re-times the three fastest, and writes the fastest
+ * tile_x, tile_y, min_blocks, pulse_chunk and stage_cap into *inout (other
  * fields kept).  The result is cached in the context under the batch's
  * shape signature (sizes and precision), so a later call with the same
  * shapes returns at once (*best_ms = -1 then).  Writes the jobs' outputs.

@@ -217,6 +217,19 @@ def test_pulse_chunk_and_launch_modes(ctx, oracle, cfg1, chunk, persistent):
     assert rel_l2(img, ref) < REL_COMPAT
 
 
+@pytest.mark.parametrize("tile,chunk,stage", [((32, 32), 64, 3264), ((32, 64), 32, 3424), ((16, 64), 128, 2944)])
+def test_two_ctas_with_grown_staging(ctx, oracle, cfg1, tile, chunk, stage):
+    """2 CTAs/SM with the staging buffer grown into the third CTA's shared
+    memory (the autotuner's 2-CTA candidates): same tolerance as above."""
+    d = cfg1
+    pos32, k32 = d["pos"].astype(np.float32), d["k_r"].astype(np.float32)
+    img = ctx.backprojection_cuda(d["phs"], k32, d["taylor"], d["N_fft"], d["delta_r"], d["u"], d["v"],
+                                  pos32, d["r"], tile=tile, pulse_chunk=chunk, min_blocks=2, stage_cap=stage)
+    ref = oracle.backprojection(d["phs"], k32, d["taylor"], d["N_fft"], d["delta_r"], pos32, d["r"],
+                                d["nu"], d["nv"], mode=oracle.MODE_REF)
+    assert rel_l2(img, ref) < REL_COMPAT
+
+
 @pytest.mark.parametrize("P,S,nu,nv", [(2, 2, 1, 1), (3, 17, 7, 13), (64, 100, 33, 65), (200, 50, 100, 3)])
 def test_ragged_sizes(ctx, oracle, P, S, nu, nv):
     """Tiny and ragged shapes: edge tiles, P and S far from powers of two,
