@@ -102,8 +102,8 @@ __device__ __forceinline__ void bulk_copy(void *dst, const void *src, uint32_t b
 // With h = s - e|d|^2 and y = e h, the exact range difference is the series
 //     Delta = h (1 + y + 2y^2 + 5y^3 + 14y^4 + ...)   (Catalan numbers)
 // MODE 0: Delta = s + e t, t = s^2 - |d|^2 (two terms); MODE 1 adds the
-// third term 2e^2 s t (on wide tiles as (e + 2e^2 s) t); MODE 2 the fourth, e^2 (-|d|^2 (h + s) + h^3 (2 + 5y))
-// over the two-term form; MODE 3 uses the closed form 2R'h / (R' + r),
+// third term 2e^2 s t (on wide tiles as (e + 2e^2 s) t); MODE 2 the
+// fourth, e^2 (-|d|^2 (h + s) + h^3 (2 + 5y)) over the two-term form; MODE 3 uses the closed form 2R'h / (R' + r),
 // r = sqrt(R'(R' - 2h)) (near field), as its nonlinear part
 // N = (s Delta - |d|^2) / (R' + r), free of the cancellation in Delta - s.
 // Narrow tiles: the records carry kappa w_hat, e' and sigma0 = kappa theta +
@@ -172,9 +172,8 @@ __device__ __forceinline__ void pulse_step(const float4 *__restrict__ rec, uint3
         } else if constexpr (MODE == 2) {
             const float2 h = __ffma2_rn(E, nd2[j], s);
             const float2 q = __ffma2_rn(__fmul2_rn(f2(5.0f), E), h, f2(2.0f));
-            // -|d|^2 (h + s) + h^3 q as h (h^2 q - |d|^2) - |d|^2 s
-            const float2 X = __ffma2_rn(h, __ffma2_rn(__fmul2_rn(h, h), q, nd2[j]), __fmul2_rn(nd2[j], s));
-            D = __ffma2_rn(EE, X, D);
+            const float2 h3 = __fmul2_rn(__fmul2_rn(h, h), h);
+            D = __ffma2_rn(EE, __ffma2_rn(h3, q, __fmul2_rn(nd2[j], __fadd2_rn(h, s))), D);
         } else if constexpr (MODE == 3) {
             float n[2];
 #pragma unroll
