@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--stage-cap", type=int, default=0)
     ap.add_argument("--min-blocks", type=int, default=0)
     ap.add_argument("--njobs", type=int, default=96, help="batch96: number of jobs")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="batch96: use --tile/--chunk/--min-blocks/--stage-cap instead of the autotuner")
     ap.add_argument("--serve-rates", default="20,50,100,200,400", help="serve: arrival rates (req/s)")
     ap.add_argument("--serve-requests", type=int, default=2000, help="serve: requests per rate")
     ap.add_argument("--serve-lanes", type=int, default=3, help="serve: concurrent batches")
@@ -467,7 +469,12 @@ def run_batch(args, rank, world, local_rank):
         return ms
 
     t0 = time.time()
-    tune, tune_ms = ctx.autotune(J)
+    if args.no_autotune:  # a fixed launch shape (profiling one shape)
+        tune = dict(tile=tuple(int(x) for x in (args.tile or "32x32").split("x")),
+                    pulse_chunk=args.chunk or 64, min_blocks=args.min_blocks or 3, stage_cap=args.stage_cap)
+        tune_ms = -1.0
+    else:
+        tune, tune_ms = ctx.autotune(J)
     tune_s = time.time() - t0
     plan = sb.Plan(ctx, J, **tune)
     for _ in range(args.warmup):
