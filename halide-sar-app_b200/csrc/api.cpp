@@ -38,19 +38,31 @@ struct PlaneAxes {
     const double *u, *v, *u_hat, *v_hat;
 };
 
-// Row slabs for a host-buffer call on one image of 2^18 pixels or more: up
-// to kMaxSlabs slabs of at least 8 tile rows, so that the positions go up and
-// the image comes down slab by slab while other slabs compute.
+// Row slabs for a host-buffer call on one image of 2^18 pixels or more, so
+// that the positions go up and the image comes down slab by slab while
+// other slabs compute: row0[0..nslabs] are tile-row boundaries.  The first
+// slab is small (1/32 of the tile rows) so that backprojection starts once
+// the phase history and a few position rows are up, the second twice that,
+// the last as small as the first so that little of the image is still to
+// come down when the kernels end; the rest in equal slabs of at least 8
+// tile rows, at most kMaxSlabs slabs in all.
 void slab_plan(const sarbp_opts *opts, int precision, int nu, int nv, int *tile_x, int *tile_y,
-               int *nslabs, int *slab_rows) {
+               int *nslabs, int (&row0)[sarbp_ctx::kMaxSlabs + 1]) {
     Runner::tile_shape(opts, tile_x, tile_y);
     const int tiles_y = (nv + *tile_y - 1) / *tile_y;
-    *nslabs = *slab_rows = 0;
-    if (precision != SARBP_PREC_NAIVE && (size_t)nu * nv >= ((size_t)1 << 18) && tiles_y >= 16) {
-        int n = std::min(sarbp_ctx::kMaxSlabs, tiles_y / 8);
-        *slab_rows = (tiles_y + n - 1) / n;
-        *nslabs = (tiles_y + *slab_rows - 1) / *slab_rows;
-    }
+    *nslabs = 0;
+    if (precision == SARBP_PREC_NAIVE || (size_t)nu * nv < ((size_t)1 << 18) || tiles_y < 16) return;
+    const int h0 = std::max(1, tiles_y / 32);
+    const int rest = tiles_y - 4 * h0;  // after the first, second and last slabs
+    const int nbody = std::max(1, std::min(sarbp_ctx::kMaxSlabs - 3, rest / 8));
+    const int hb = (rest + nbody - 1) / nbody;
+    int n = 0, y = 0;
+    row0[n++] = 0;
+    row0[n++] = y += h0;
+    row0[n++] = y += 2 * h0;
+    for (int b = 0; b < nbody && y < tiles_y - h0; ++b) row0[n++] = y = std::min(tiles_y - h0, y + hb);
+    row0[n++] = tiles_y;
+    *nslabs = n - 1;
 }
 
 // Copies host arrays to one device block, runs one job, copies the image back.
@@ -91,8 +103,8 @@ int run_host_job(sarbp_ctx *ctx, const float *phs, int S, int P, const float *k_
     cudaStream_t st = ctx->stream;
     // Row slabs: the pixel positions go up and the image comes down slab by
     // slab while other slabs compute (images of 2^18 pixels and more).
-    int tile_x = 0, tile_y = 0, nslabs = 0, slab_rows = 0;
-    slab_plan(opts, precision, nu, nv, &tile_x, &tile_y, &nslabs, &slab_rows);
+    int tile_x = 0, tile_y = 0, nslabs = 0, row0[sarbp_ctx::kMaxSlabs + 1] = {};
+    slab_plan(opts, precision, nu, nv, &tile_x, &tile_y, &nslabs, row0);
     cudaStream_t cin = nslabs ? ctx->copy_in : st;
     struct Copy { void *dst; const void *src; size_t n; };
     const Copy copies[] = {
@@ -117,8 +129,8 @@ int run_host_job(sarbp_ctx *ctx, const float *phs, int S, int P, const float *k_
         // and range compression are enqueued (see SlabSpec::before_slabs)
         spec.before_slabs = [&]() -> cudaError_t {
             for (int g = 0; g < nslabs && r; ++g) {
-                const size_t y0 = (size_t)g * slab_rows * tile_y;
-                const size_t y1 = std::min((size_t)nv, (size_t)(g + 1) * slab_rows * tile_y);
+                const size_t y0 = std::min((size_t)nv, (size_t)row0[g] * tile_y);
+                const size_t y1 = std::min((size_t)nv, (size_t)row0[g + 1] * tile_y);
                 for (int c = 0; c < 3 && y1 > y0; ++c) {
                     const size_t off = (size_t)c * npix + y0 * (size_t)nu;
                     cudaError_t ce = cudaMemcpyAsync(d_r + off, r + off, (y1 - y0) * (size_t)nu * sizeof(double),
@@ -131,7 +143,7 @@ int run_host_job(sarbp_ctx *ctx, const float *phs, int S, int P, const float *k_
             return cudaSuccess;
         };
         spec.nslabs = nslabs;
-        spec.tile_rows = slab_rows;
+        spec.row0 = row0;
         spec.aux = ctx->aux;
         spec.ready = r ? ctx->ev_ready : nullptr;
         spec.done = ctx->ev_done;
@@ -175,8 +187,8 @@ int run_host_job(sarbp_ctx *ctx, const float *phs, int S, int P, const float *k_
     // output rows are flipped (backprojection.cpp:130): pixel rows [y0, y1)
     // are image rows [nv - y1, nv - y0)
     for (int g = 0; g < nslabs; ++g) {
-        const size_t y0 = (size_t)g * slab_rows * tile_y;
-        const size_t y1 = std::min((size_t)nv, (size_t)(g + 1) * slab_rows * tile_y);
+        const size_t y0 = std::min((size_t)nv, (size_t)row0[g] * tile_y);
+        const size_t y1 = std::min((size_t)nv, (size_t)row0[g + 1] * tile_y);
         if ((e = cudaStreamWaitEvent(ctx->copy_out, ctx->ev_done[g], 0)) != cudaSuccess)
             return cuda_fail(e, "cudaStreamWaitEvent");
         const size_t off = ((size_t)nv - y1) * (size_t)nu * 2;

@@ -20,7 +20,7 @@ struct sarbp_ctx {
     std::map<std::string, sarbp_opts> tuned;  // autotuner results by job-set key
     // host-buffer entry points: copies in, second compute stream, copies out,
     // and the events that pipeline row slabs between them
-    static constexpr int kMaxSlabs = 8;
+    static constexpr int kMaxSlabs = 12;
     cudaStream_t copy_in = nullptr, aux = nullptr, copy_out = nullptr;
     cudaEvent_t ev_out = nullptr;
     cudaEvent_t ev_ready[kMaxSlabs] = {}, ev_done[kMaxSlabs] = {};

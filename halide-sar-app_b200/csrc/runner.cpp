@@ -234,7 +234,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
                     void *q_out, bool for_graph, const SlabSpec *slabs) {
     const bool rc_only = q_out != nullptr;
     if (slabs && slabs->nslabs > 0) {
-        if (njobs != 1 || rc_only || for_graph || slabs->tile_rows < 1 || !slabs->aux || !slabs->done)
+        if (njobs != 1 || rc_only || for_graph || !slabs->row0 || !slabs->aux || !slabs->done)
             return fail(SARBP_ERR_INVALID, "row slabs need one job, a second stream and done events");
         if (!front_done_) {
             cudaError_t e = cudaEventCreateWithFlags(&front_done_, cudaEventDisableTiming);
@@ -470,8 +470,8 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         const int tiles_x = (jobs[0].nu + L.tile_x - 1) / L.tile_x;
         if (bp_max_active_blocks(L) < 1) return fail(SARBP_ERR_CUDA, "backprojection kernel does not fit on an SM");
         for (int g = 0; g < slabs->nslabs; ++g) {
-            const size_t first = std::min(items.size(), (size_t)g * slabs->tile_rows * tiles_x);
-            const size_t last = std::min(items.size(), (size_t)(g + 1) * slabs->tile_rows * tiles_x);
+            const size_t first = std::min(items.size(), (size_t)slabs->row0[g] * tiles_x);
+            const size_t last = std::min(items.size(), (size_t)std::max(slabs->row0[g], slabs->row0[g + 1]) * tiles_x);
             cudaStream_t sg = (g & 1) ? slabs->aux : st;
             if ((g & 1) && (e = cudaStreamWaitEvent(sg, front_done_, 0)) != cudaSuccess)
                 return cuda_fail(e, "cudaStreamWaitEvent");

@@ -62,7 +62,7 @@ struct DeviceInfo {
 };
 
 // Row slabs of a single job, for overlapping its host<->device copies with
-// compute: slab g covers tile rows [g * tile_rows, (g + 1) * tile_rows).
+// compute: slab g covers tile rows [row0[g], row0[g + 1]).
 // After prep and range compression (on the main stream), slab g's tile
 // geometry and backprojection run on the main stream (g even) or `aux`
 // (g odd) once `ready[g]` has fired (when set), and `done[g]` is recorded
@@ -71,7 +71,7 @@ struct DeviceInfo {
 // the SMs while the previous slab's last tiles finish.
 struct SlabSpec {
     int nslabs = 0;
-    int tile_rows = 0;
+    const int *row0 = nullptr;  // [nslabs + 1] tile-row boundaries, ascending
     cudaStream_t aux = nullptr;
     const cudaEvent_t *ready = nullptr;  // [nslabs] or NULL
     const cudaEvent_t *done = nullptr;   // [nslabs]

@@ -443,5 +443,5 @@ def test_kernels_are_launched(ctx, cfg1):
                             d["u"], d["v"], d["pos"].astype(np.float32), d["r"])
     # set-up and range compression, then tile geometry (with the pulse
     # records) and backprojection per row slab: 512 x 512 in 32-row tiles is
-    # 16 tile rows, pipelined as 2 slabs of 8
-    assert ctx.launch_count() - before == 2 + 2 * 2
+    # 16 tile rows, pipelined as 4 slabs of 1, 2, 12 and 1 tile rows
+    assert ctx.launch_count() - before == 2 + 2 * 4
