@@ -40,7 +40,7 @@ FP32_PER_UNIT = 18  # FP32-pipe instructions per pixel*pulse (algorithmic)
 SFU_PER_UNIT = 3    # SFU operations per pixel*pulse (algorithmic)
 # DRAM bytes (read + write) of one bp_tile_kernel launch, from an ncu capture
 # of the default plain_large step (profiles/bp_tile_kernel_32x32_plain_large_2048x1999.md)
-NCU_BP_TRAFFIC = {"plain_large": 576.083968e6 + 84.414464e6}
+NCU_BP_TRAFFIC = {"plain_large": 571.163392e6 + 82.052096e6}
 
 
 def parse():

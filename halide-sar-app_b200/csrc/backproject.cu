@@ -224,7 +224,7 @@ __device__ __forceinline__ void accumulate(int nc, const float4 *__restrict__ re
                                            const float2 (&dx)[NP], const float2 (&dy)[NP],
                                            const float2 (&dz)[NP], const float2 (&nd2)[NP],
                                            const float2 (&s0)[NP], float2 (&ar)[NP], float2 (&ai)[NP]) {
-#pragma unroll 4
+#pragma unroll 6
     for (int i = 0; i < nc; ++i, poff += pstride)
         pulse_step<MODE, PLANAR, WIDE, NP>(rec2 + 4 * i, poff, ILK, CL, dx, dy, dz, nd2, s0, ar, ai);
 }
