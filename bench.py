@@ -38,8 +38,11 @@ sys.path.insert(0, os.path.join(ROOT, "halide-sar-app_b200"))
 
 FP32_PER_UNIT = 18  # FP32-pipe instructions per pixel*pulse (algorithmic)
 SFU_PER_UNIT = 3    # SFU operations per pixel*pulse (algorithmic)
+U8_LAUNCHES = 50    # back-to-back calls the output stage is timed over
+SERVE_RATES = (100.0, 200.0, 400.0)  # req/s of the serving block of the default run
+SERVE_REQUESTS = 400                 # requests per rate there
 # DRAM bytes (read + write) of one bp_tile_kernel launch, from an ncu capture
-# of the default plain_large step (profiles/bp_tile_kernel_32x32_plain_large_2048x1999.md)
+# (dram__bytes_read.sum + dram__bytes_write.sum) of the default plain_large step
 NCU_BP_TRAFFIC = {"plain_large": 571.163392e6 + 82.052096e6}
 
 
@@ -55,6 +58,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer timing (profiling)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="plain_large: skip the batch96 and serving blocks (profiling)")
     ap.add_argument("--tile", default="", help="e.g. 32x32")
     ap.add_argument("--chunk", type=int, default=0)
     ap.add_argument("--stage-cap", type=int, default=0)
@@ -300,15 +305,14 @@ def run_ours(args, rank, world, local_rank):
         ms_max = float(t.item())
     value = world * units * args.steps / (ms_max * 1e-3) / 1e9
 
-    # output stage (dB + u8), outside the step: HBM-bound tail
+    # output stage (max|z| + u8 of the complex image), outside the step: the
+    # HBM-bound tail, timed over U8_LAUNCHES back-to-back calls
     t_u8 = torch.empty((nv, nu), dtype=torch.uint8, device=dev)
-    job_u8 = sb.make_job(S, P, data["N_fft"], data["taylor"], nu, nv, data["delta_r"], t_phs.data_ptr(),
-                         t_k.data_ptr(), t_pos.data_ptr(), t_out.data_ptr(), r=t_r.data_ptr(),
-                         out_u8=t_u8.data_ptr(), dB_min=data["db"][0], dB_max=data["db"][1])
-    u8_ms = []
+    u8_call = lambda: ctx.img_output_u8_from_img_device(t_out.data_ptr(), nu, nv, data["db"][0],
+                                                        data["db"][1], t_u8.data_ptr())
     for _ in range(3):
-        ctx.run_jobs([job_u8], **tune)
-        u8_ms.append(ctx.last_stage_ms()[4])
+        u8_call()
+    u8_ms = timed_ms(torch, stream, u8_call, U8_LAUNCHES) / U8_LAUNCHES
     ctx.synchronize()
 
     # ---- e2e through the host-buffer entry point, pinned host memory ----
@@ -364,7 +368,7 @@ def run_ours(args, rank, world, local_rank):
     else:
         achieved, peak = FP32_PER_UNIT * bp_units_s / 1e12, ffma_s / 1e12
     rc_bytes = P * S * 8 + P * data["N_fft"] * 8
-    u8_bytes = nu * nv * (16 + 1)
+    u8_bytes = nu * nv * (16 + 16 + 1)  # max|z| pass, then image in and u8 out
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -381,7 +385,7 @@ def run_ours(args, rank, world, local_rank):
         "config": config_block(data, world),
         "gpu_launches": int(launches),
         "stage_ms": {"setup": prep_ms, "range_compress": rc_ms, "tile_geometry": geom_ms, "backproject": bp_ms,
-                     "db_u8": float(np.mean(u8_ms))},
+                     "db_u8": u8_ms},
         "roofline": {"bound": bound, "achieved": achieved, "peak": peak, "unit": "Tops/s",
                      "frac": achieved / peak,
                      "traffic": NCU_BP_TRAFFIC.get(args.config) if default_launch else None,
@@ -397,9 +401,11 @@ def run_ours(args, rank, world, local_rank):
                                "peak": hbm_peak, "unit": "GB/s",
                                "frac": rc_bytes / (rc_ms * 1e-3) / 1e9 / hbm_peak,
                                "bytes": rc_bytes},
-            "db_u8": {"bound": "hbm", "achieved": u8_bytes / (np.mean(u8_ms) * 1e-3) / 1e9,
+            "db_u8": {"bound": "hbm", "achieved": u8_bytes / (u8_ms * 1e-3) / 1e9,
                       "peak": hbm_peak, "unit": "GB/s",
-                      "frac": u8_bytes / (np.mean(u8_ms) * 1e-3) / 1e9 / hbm_peak, "bytes": u8_bytes},
+                      "frac": u8_bytes / (u8_ms * 1e-3) / 1e9 / hbm_peak, "bytes": u8_bytes,
+                      "how": "sarbp_img_output_u8_from_img_device (max|z| kernel + u8 kernel), "
+                             "%d back-to-back calls" % U8_LAUNCHES},
             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s"},
         "e2e": {"value": e2e_value, "unit": "Gpixel*pulses/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms / max(args.e2e_steps, 1),
@@ -414,6 +420,23 @@ def run_ours(args, rank, world, local_rank):
                                          "%d threads, %.1f s; range compression of all pulses "
                                          "charged pro rata)" % (cb["n_pix"], P, cb["cores"],
                                                                 cb["seconds"])}
+    if world == 1 and args.config == "plain_large" and not args.no_extras:
+        # the rest of the headline metric: the batched form (ratio to the
+        # plain single image above) and the serving loop (p50/p99 and the
+        # FP64 rel-L2 of a 5 % request sample), bounded to about a minute
+        b = batch_measure(torch, ctx, stream, dev, 96, 7, steps=5, warmup=3, e2e_steps=1, full=False)
+        out["batch96"] = {
+            "metric": "Gpixel*pulses/s (96 uneven jobs, one persistent launch, CUDA-graph replay)",
+            "value": b["value"], "unit": "Gpixel*pulses/s", "ms_per_step": b["ms_per_step"],
+            "steps": b["steps"], "workload": b["workload"], "gpu_launches": b["gpu_launches"],
+            "ratio_to_plain_single_image": b["value"] / value,
+            "ratio_to_loop_of_per_image_calls": b["compare"]["speedup_vs_loop"],
+            "compare": b["compare"], "autotuned": b["autotuned"], "l2": b["l2"], "clocks": b["clocks"]}
+        s = serve_measure(torch, ctx, dev, SERVE_RATES, SERVE_REQUESTS, 3, 0.0, 7)
+        out["serve"] = {"metric": "serving latency p50/p99 (ms) and throughput under Poisson arrivals",
+                        "sweep": s["sweep"], "fp64_sample": s["fp64_sample"], "residency": s["residency"],
+                        "peak_device_bytes": s["peak_device_bytes"], "workload": s["workload"],
+                        "latency": s["latency"], "clocks": s["clocks"]}
     ctx.close()
     if rank == 0:
         print(json.dumps(out), flush=True)
@@ -431,35 +454,154 @@ def timed_ms(torch, stream, fn, steps):
     return e0.elapsed_time(e1)
 
 
-def run_batch(args, rank, world, local_rank):
-    """batch96: 96 uneven image-formation jobs (images 256^2..2048^2, 128-2000
-    pulses, 256-1024 samples, 5-15 km, 20-50 deg) formed together: one
-    autotuned persistent launch sequence replayed as a CUDA graph.  Compared
-    in the same run with the same jobs as (a) one batched call without the
-    graph, (b) a loop of plain per-image calls, (c) a loop of per-image calls
-    of the plain FP32 kernel (PREC_NAIVE)."""
-    import torch
-    import torch.distributed as dist
+def batch_measure(torch, ctx, stream, dev, njobs, seed, steps, warmup, e2e_steps, tune=None,
+                  lanes=3, batch_work=0.0, gmax=lambda ms: ms, full=True):
+    """The batched form: `njobs` uneven image-formation jobs (images
+    256^2..2048^2, 128-2000 pulses, 256-1024 samples, Taylor 17-35 dB, 5-15 km,
+    20-50 deg) formed together in one autotuned persistent launch sequence
+    replayed as a CUDA graph.  Compared with the same jobs as one batched call
+    without the graph and as a loop of per-image calls of the split-precision
+    kernel; with `full`, also a loop of per-image calls of the plain FP32
+    kernel (PREC_NAIVE) and the e2e figures from host memory."""
     import sarbp_b200 as sb
     from sarbp_b200 import synth
-    from sarbp_b200.batch import DeviceJob
+    from sarbp_b200.batch import DeviceJob, HostJob
 
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
     t0 = time.time()
-    cfgs = synth.batch_jobs(njobs=args.njobs, seed=7 + rank)
+    cfgs = synth.batch_jobs(njobs=njobs, seed=seed)
     jobs = [DeviceJob(c, torch, dev) for c in cfgs]
     synth_s = time.time() - t0
     units = float(sum(j.units for j in jobs))
     J = [j.job for j in jobs]
+    sp = stream.cuda_stream
+    t0 = time.time()
+    if tune is not None:  # a fixed launch shape (profiling one shape)
+        tune_ms = -1.0
+    else:
+        tune, tune_ms = ctx.autotune(J)
+    tune_s = time.time() - t0
+    plan = sb.Plan(ctx, J, **tune)
+    for _ in range(warmup):
+        plan.launch(sp)
+    plan.wait()
+    clocks = Clocks(gpu_uuid(torch, dev))
+    clocks.start()
+    n0 = ctx.launch_count()
+    ms_graph = gmax(timed_ms(torch, stream, lambda: plan.launch(sp), steps))
+    launches = ctx.launch_count() - n0
+    plan.wait()
+    clk = clocks.stop()
+    k2 = max(1, steps // 2) if full else 1
+    ms_batch = gmax(timed_ms(torch, stream, lambda: ctx.run_jobs(J, **tune), k2))
+    ctx.synchronize()
+    ms_loop = gmax(timed_ms(torch, stream, lambda: [ctx.run_jobs([j]) for j in J], k2))
+    ctx.synchronize()
+    g = lambda ms, k: units * k / (ms * 1e-3) / 1e9
+    res = {
+        "value": g(ms_graph, steps), "ms_per_step": ms_graph / steps, "steps": steps,
+        "pixel_pulses_per_step": units, "gpu_launches": int(launches),
+        "workload": "%d jobs, images %s, pulses %d-%d, samples %s, Taylor %d-%d dB "
+                    "(float-quotient window above 30 dB)"
+                    % (len(jobs), "/".join("%dx%d" % s for s in sorted(set((j.nu, j.nv) for j in jobs))),
+                       min(j.P for j in jobs), max(j.P for j in jobs),
+                       "/".join(str(s) for s in sorted(set(j.S for j in jobs))),
+                       min(c["taylor"] for c in cfgs), max(c["taylor"] for c in cfgs)),
+        "autotuned": {"tile": list(tune["tile"]), "pulse_chunk": tune["pulse_chunk"],
+                      "stage_cap": tune.get("stage_cap", 0), "min_blocks": tune["min_blocks"],
+                      "best_ms": tune_ms, "seconds": tune_s},
+        "compare": {"graph_replay": g(ms_graph, steps),
+                    "batched_call_no_graph": g(ms_batch, k2),
+                    "loop_of_per_image_calls": g(ms_loop, k2),
+                    "speedup_vs_loop": ms_loop / k2 / (ms_graph / steps)},
+        "l2": "inputs+outputs %.1f GB per step (> 126 MB L2), no flush"
+              % (sum(j.device_bytes() for j in jobs) / 1e9),
+        "clocks": clk, "synthesis_seconds": synth_s,
+    }
+    if full:
+        ms_naive = gmax(timed_ms(torch, stream,
+                                 lambda: [ctx.run_jobs([j], precision=sb.PREC_NAIVE) for j in J], 1))
+        ctx.synchronize()
+        res["compare"]["loop_of_per_image_naive_fp32"] = g(ms_naive, 1)
+        res["compare"]["speedup_vs_naive_loop"] = ms_naive / (ms_graph / steps)
+        # end to end: phase histories, k_r, pos from pinned host memory in,
+        # the complex images out, around each graph replay (one stream)
+        h_in = [(t, t.cpu().pin_memory()) for j in jobs for t in (j.phs, j.k_r, j.pos)]
+        h_out = [(j.out, torch.empty(j.out.shape, dtype=j.out.dtype).pin_memory()) for j in jobs]
+
+        def e2e_step():
+            for d, h in h_in:
+                d.copy_(h, non_blocking=True)
+            plan.launch(sp)
+            for d, h in h_out:
+                h.copy_(d, non_blocking=True)
+
+        e2e_step()
+        plan.wait()
+        ms_e2e = gmax(timed_ms(torch, stream, e2e_step, e2e_steps))
+        plan.wait()
+        res["e2e_graph_serial_copies"] = {
+            "value": g(ms_e2e, e2e_steps), "unit": "Gpixel*pulses/s",
+            "h2d_bytes_per_step": int(sum(h.numel() * h.element_size() for _, h in h_in)),
+            "d2h_bytes_per_step": int(sum(h.numel() * h.element_size() for _, h in h_out)),
+            "ms_per_step": ms_e2e / e2e_steps, "steps": e2e_steps,
+            "how": "inputs copied in, graph replayed, images copied out, one stream"}
+        del h_in, h_out
+    plan.close()
+    if full:
+        # end to end through the serving loop: the same jobs in pinned host
+        # memory submitted at once, complex images back in pinned host
+        # memory; a step is first submission -> last image on the host
+        pin = lambda shape, dtype: torch.empty(
+            shape, dtype=getattr(torch, np.dtype(dtype).name)).pin_memory().numpy()
+        hjobs = [HostJob(j.cfg, alloc=pin, data=j.data) for j in jobs]
+        houts = [hj.new_outputs()[0] for hj in hjobs]
+        srv = sb.Server(ctx, hbm_cap_bytes=150e9, lanes=lanes, max_batch=32, max_batch_work=batch_work,
+                        precision=sb.PREC_COMPAT)
+
+        def burst():
+            rids = [srv.submit(hj.job(o, precision=sb.PREC_COMPAT)) for hj, o in zip(hjobs, houts)]
+            first = last = None
+            for r in rids:
+                rc = srv.wait(r)
+                if rc != 0:
+                    raise RuntimeError("request failed: %d %s" % (rc, sb.last_error()))
+                ts, _, td = srv.times(r)
+                first = ts if first is None else min(first, ts)
+                last = td if last is None else max(last, td)
+                srv.release(r)
+            return (last - first) * 1e3
+
+        try:
+            burst()
+            b0 = srv.stats()["batches"]
+            ms_srv = gmax(sum(burst() for _ in range(e2e_steps)))
+            srv_batches = (srv.stats()["batches"] - b0) / e2e_steps
+        finally:
+            srv.close()
+        res["e2e"] = {
+            "value": g(ms_srv, e2e_steps), "unit": "Gpixel*pulses/s",
+            "h2d_bytes_per_step": int(sum(hj.phs.nbytes + hj.k32.nbytes + hj.p32.nbytes + hj.u.nbytes
+                                          + hj.v.nbytes for hj in hjobs)),
+            "d2h_bytes_per_step": int(sum(o.nbytes for o in houts)),
+            "ms_per_step": ms_srv / e2e_steps, "steps": e2e_steps, "batches_per_step": srv_batches,
+            "lanes": lanes,
+            "how": "all jobs submitted at once to the serving loop (sarbp_server_*) from pinned "
+                   "host memory; first submission to last image on the host"}
+    res["tune"] = tune
+    return res
+
+
+def run_batch(args, rank, world, local_rank):
+    """--config batch96: the batched form on its own (see batch_measure)."""
+    import torch
+    import torch.distributed as dist
+    import sarbp_b200 as sb
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
     ctx = sb.Context(local_rank)
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
-    sp = stream.cuda_stream
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
 
     def gmax(ms):
         if world > 1:
@@ -468,177 +610,105 @@ def run_batch(args, rank, world, local_rank):
             ms = float(t.item())
         return ms
 
-    t0 = time.time()
-    if args.no_autotune:  # a fixed launch shape (profiling one shape)
+    tune = None
+    if args.no_autotune:
         tune = dict(tile=tuple(int(x) for x in (args.tile or "32x32").split("x")),
                     pulse_chunk=args.chunk or 64, min_blocks=args.min_blocks or 3, stage_cap=args.stage_cap)
-        tune_ms = -1.0
-    else:
-        tune, tune_ms = ctx.autotune(J)
-    tune_s = time.time() - t0
-    plan = sb.Plan(ctx, J, **tune)
-    for _ in range(args.warmup):
-        plan.launch(sp)
-    plan.wait()
-    clocks = Clocks(gpu_uuid(torch, dev)) if rank == 0 else None
-    if clocks:
-        clocks.start()
-    barrier()
-    n0 = ctx.launch_count()
-    ms_graph = gmax(timed_ms(torch, stream, lambda: plan.launch(sp), args.steps))
-    launches = ctx.launch_count() - n0
-    plan.wait()
-    clk = clocks.stop() if clocks else {}
-    k2 = max(1, args.steps // 2)
-    ms_batch = gmax(timed_ms(torch, stream, lambda: ctx.run_jobs(J, **tune), k2))
-    ctx.synchronize()
-    ms_loop = gmax(timed_ms(torch, stream, lambda: [ctx.run_jobs([j]) for j in J], k2))
-    ctx.synchronize()
-    ms_naive = gmax(timed_ms(torch, stream, lambda: [ctx.run_jobs([j], precision=sb.PREC_NAIVE) for j in J], 1))
-    ctx.synchronize()
-
-    # end to end: phase histories, k_r, pos from pinned host memory in, the
-    # complex images out, around each graph replay
-    h_in = [(t, t.cpu().pin_memory()) for j in jobs for t in (j.phs, j.k_r, j.pos)]
-    h_out = [(j.out, torch.empty(j.out.shape, dtype=j.out.dtype).pin_memory()) for j in jobs]
-
-    def e2e_step():
-        for d, h in h_in:
-            d.copy_(h, non_blocking=True)
-        plan.launch(sp)
-        for d, h in h_out:
-            h.copy_(d, non_blocking=True)
-
-    e2e_step()
-    plan.wait()
-    e2e_steps = max(1, min(args.e2e_steps, args.steps))
-    ms_e2e = gmax(timed_ms(torch, stream, e2e_step, e2e_steps))
-    plan.wait()
-    h2d = sum(h.numel() * h.element_size() for _, h in h_in)
-    d2h = sum(h.numel() * h.element_size() for _, h in h_out)
-    plan.close()
-    del h_in, h_out
-
-    # end to end through the serving loop: the same jobs in pinned host
-    # memory submitted at once, complex images back in pinned host memory;
-    # a step is first submission -> last image on the host (server clock)
-    from sarbp_b200.batch import HostJob
-    pin = lambda shape, dtype: torch.empty(shape, dtype=getattr(torch, np.dtype(dtype).name)).pin_memory().numpy()
-    hjobs = [HostJob(j.cfg, alloc=pin, data=j.data) for j in jobs]
-    houts = [hj.new_outputs()[0] for hj in hjobs]
-    srv = sb.Server(ctx, hbm_cap_bytes=150e9, lanes=args.serve_lanes, max_batch=32,
-                    max_batch_work=args.serve_batch_work, precision=sb.PREC_COMPAT)
-
-    def burst():
-        rids = [srv.submit(hj.job(o, precision=sb.PREC_COMPAT)) for hj, o in zip(hjobs, houts)]
-        first = last = None
-        for r in rids:
-            rc = srv.wait(r)
-            if rc != 0:
-                raise RuntimeError("request failed: %d %s" % (rc, sb.last_error()))
-            ts, _, td = srv.times(r)
-            first = ts if first is None else min(first, ts)
-            last = td if last is None else max(last, td)
-            srv.release(r)
-        return (last - first) * 1e3
-
-    try:
-        burst()
-        b0 = srv.stats()["batches"]
-        ms_srv = gmax(sum(burst() for _ in range(e2e_steps)))
-        srv_batches = (srv.stats()["batches"] - b0) / e2e_steps
-    finally:
-        srv.close()
-    srv_h2d = sum(hj.phs.nbytes + hj.k32.nbytes + hj.p32.nbytes + hj.u.nbytes + hj.v.nbytes for hj in hjobs)
-    srv_d2h = sum(o.nbytes for o in houts)
-
-    g = lambda ms, k: world * units * k / (ms * 1e-3) / 1e9
-    sizes = sorted(set((j.nu, j.nv) for j in jobs))
+    if world > 1:
+        dist.barrier()
+    r = batch_measure(torch, ctx, stream, dev, args.njobs, 7 + rank, args.steps, args.warmup,
+                      max(1, min(args.e2e_steps, args.steps)), tune=tune, lanes=args.serve_lanes,
+                      batch_work=args.serve_batch_work, gmax=gmax, full=True)
+    ctx.close()
     out = {
         "metric": "Gpixel*pulses/s (96 uneven jobs, batched)",
-        "value": g(ms_graph, args.steps), "unit": "Gpixel*pulses/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_graph / args.steps,
+        "value": world * r["value"], "unit": "Gpixel*pulses/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 (split-precision; f64 per-pulse set-up)",
         "data": "synthetic (seeded uneven jobs)",
-        "config": {"workload": "batch96: %d jobs, images %s, pulses %d-%d, samples %s, Taylor %d-%d dB"
-                               % (len(jobs), "/".join("%dx%d" % s for s in sizes),
-                                  min(j.P for j in jobs), max(j.P for j in jobs),
-                                  "/".join(str(s) for s in sorted(set(j.S for j in jobs))),
-                                  min(c["taylor"] for c in cfgs), max(c["taylor"] for c in cfgs)),
-                   "pixel_pulses_per_step": units, "precision": "compat",
-                   "parallelism": "replicas%d" % world,
-                   "l2": "inputs+outputs %.1f GB per step (> 126 MB L2), no flush"
-                         % (sum(j.device_bytes() for j in jobs) / 1e9)},
-        "gpu_launches": int(launches),
-        "autotuned": {"tile": list(tune["tile"]), "pulse_chunk": tune["pulse_chunk"],
-                      "stage_cap": tune.get("stage_cap", 0),
-                      "min_blocks": tune["min_blocks"], "best_ms": tune_ms, "seconds": tune_s},
-        "compare": {
-            "graph_replay": g(ms_graph, args.steps),
-            "batched_call_no_graph": g(ms_batch, k2),
-            "loop_of_per_image_calls": g(ms_loop, k2),
-            "loop_of_per_image_naive_fp32": g(ms_naive, 1),
-            "speedup_vs_loop": ms_loop / k2 / (ms_graph / args.steps),
-            "speedup_vs_naive_loop": ms_naive / (ms_graph / args.steps)},
-        # host-resident jobs go through the serving loop (copies of one
-        # batch overlap the kernels of the others)
-        "e2e": {"value": g(ms_srv, e2e_steps), "unit": "Gpixel*pulses/s",
-                "h2d_bytes_per_step": int(srv_h2d), "d2h_bytes_per_step": int(srv_d2h),
-                "ms_per_step": ms_srv / e2e_steps, "steps": e2e_steps,
-                "batches_per_step": srv_batches, "lanes": args.serve_lanes,
-                "how": "all jobs submitted at once to the serving loop (sarbp_server_*) from pinned "
-                       "host memory; first submission to last image on the host"},
-        "e2e_graph_serial_copies": {
-            "value": g(ms_e2e, e2e_steps), "unit": "Gpixel*pulses/s", "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e / e2e_steps, "steps": e2e_steps,
-            "how": "inputs copied in, graph replayed, images copied out, one stream"},
-        "clocks": clk,
-        "synthesis_seconds": synth_s,
+        "config": {"workload": "batch96: " + r["workload"],
+                   "pixel_pulses_per_step": r["pixel_pulses_per_step"], "precision": "compat",
+                   "parallelism": "replicas%d" % world, "l2": r["l2"]},
+        "gpu_launches": r["gpu_launches"], "autotuned": r["autotuned"], "compare": r["compare"],
+        "e2e": dict(r["e2e"], value=world * r["e2e"]["value"]),
+        "e2e_graph_serial_copies": r["e2e_graph_serial_copies"],
+        "clocks": r["clocks"], "synthesis_seconds": r["synthesis_seconds"],
     }
-    ctx.close()
     if rank == 0:
         print(json.dumps(out), flush=True)
 
 
-def run_serve(args, rank, world, local_rank):
-    """serve: the serving loop under Poisson arrivals.  A pool of 96 uneven
-    jobs (the batch96 distribution) lives in pinned host memory; each request
-    picks one (seeded), is submitted at its arrival time and returns its
-    complex image to pinned host memory.  Latency is submission to
-    image-on-host on the server's clock; p50/p99 over --serve-requests
-    requests per rate.  PREC_PRECISE (f64 positions and k_r)."""
-    import torch
+def fp64_sample_rel_l2(pool, picks, seed, pixels=1000):
+    """rel-L2 vs the FP64 oracle of the served images of the sampled requests
+    (pool job k, image) at `pixels` random pixels each."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.lib()
+    rng = np.random.default_rng(seed)
+    errs = []
+    for k, img in picks:
+        hj = pool[k]
+        d = hj.data
+        r = O.pixel_locs(d["u"], d["v"], d["u_hat"], d["v_hat"])
+        idx = rng.choice(hj.nu * hj.nv, min(pixels, hj.nu * hj.nv), replace=False)
+        ref = O.backprojection(d["phs"], d["k_r"], d["taylor"], d["N_fft"], d["delta_r"], d["pos"], r,
+                               hj.nu, hj.nv, mode=O.MODE_FP64, out_idx=idx,
+                               taylor_mode=d.get("taylor_mode", 0))
+        got = img.ravel()[idx]
+        errs.append(float(np.linalg.norm(got - ref) / np.linalg.norm(ref)))
+    return errs
+
+
+def serve_measure(torch, ctx, dev, rates, nreq, lanes, batch_work, seed, sample_frac=0.05, resident=True):
+    """The serving loop under Poisson arrivals.  A pool of 96 uneven jobs (the
+    batch96 distribution) lives in pinned host memory; with `resident` their
+    phase histories are registered once (uploaded and range-compressed
+    once, kept on the device) and each request brings only its image plane;
+    each request picks a pool job (seeded), is submitted at its arrival time
+    and returns its complex image to pinned host memory.  Latency is
+    submission to image-on-host on the server's clock; p50/p99 over `nreq`
+    requests per rate.  PREC_PRECISE (f64 positions and k_r).  A seeded
+    `sample_frac` of the requests keep their own output buffers and are
+    checked against the FP64 oracle afterwards, outside the timed sweep."""
     import sarbp_b200 as sb
     from sarbp_b200 import synth
     from sarbp_b200.batch import HostJob
 
-    torch.cuda.set_device(local_rank)
     pin = lambda shape, dtype: torch.empty(shape, dtype=getattr(torch, np.dtype(dtype).name)).pin_memory().numpy()
-    cfgs = synth.batch_jobs(njobs=96, seed=7 + rank)
+    cfgs = synth.batch_jobs(njobs=96, seed=seed)
     t0 = time.time()
     pool = [HostJob(c, alloc=pin) for c in cfgs]
-    outs = [hj.new_outputs()[0] for hj in pool]  # one image buffer per pool job (same image each time)
+    outs = [hj.new_outputs()[0] for hj in pool]  # shared image buffer per pool job
     synth_s = time.time() - t0
-    ctx = sb.Context(local_rank)
-    rates = [float(x) for x in args.serve_rates.split(",")]
-    nreq = args.serve_requests
-    clocks = Clocks(gpu_uuid(torch, torch.device("cuda", local_rank))) if rank == 0 else None
-    sweep = []
-    srv = sb.Server(ctx, hbm_cap_bytes=150e9, lanes=args.serve_lanes, max_batch=32,
-                    max_batch_work=args.serve_batch_work, precision=sb.PREC_PRECISE)
+    clocks = Clocks(gpu_uuid(torch, dev))
+    sweep, picks = [], []
+    srng = np.random.default_rng(seed + 99)
+    srv = sb.Server(ctx, hbm_cap_bytes=150e9, lanes=lanes, max_batch=32, max_batch_work=batch_work,
+                    precision=sb.PREC_PRECISE)
+    ap = [None] * len(pool)
+    reg_s = 0.0
     try:
-        # warm-up: every pool job once
-        for k in range(len(pool)):
-            r = srv.submit(pool[k].job(outs[k], precision=sb.PREC_PRECISE))
+        if resident:  # phase histories uploaded and range-compressed once
+            t0 = time.time()
+            ap = [srv.register(hj.job(outs[k], precision=sb.PREC_PRECISE)) for k, hj in enumerate(pool)]
+            reg_s = time.time() - t0
+
+        def submit(k, o):
+            job = pool[k].job(o, precision=sb.PREC_PRECISE)
+            return srv.submit_on(ap[k], job) if resident else srv.submit(job)
+
+        for k in range(len(pool)):  # warm-up: every pool job once
+            r = submit(k, outs[k])
             srv.wait(r)
             srv.release(r)
-        if clocks:
-            clocks.start()
+        c0 = srv.counters()
+        clocks.start()
         for rate in rates:
-            rng = np.random.default_rng(int(rate * 1000) + rank)
+            rng = np.random.default_rng(int(rate * 1000) + seed)
             pick = rng.integers(0, len(pool), nreq)
             arrive = np.cumsum(rng.exponential(1.0 / rate, nreq))
+            own = set(srng.choice(nreq, max(1, int(round(sample_frac * nreq))), replace=False).tolist())
             b0 = srv.stats()["batches"]
             rids = []
             start = time.perf_counter()
@@ -649,9 +719,10 @@ def run_serve(args, rank, world, local_rank):
                         break
                     time.sleep(dt if dt > 2e-3 else 0)
                 k = int(pick[i])
-                rids.append((srv.submit(pool[k].job(outs[k], precision=sb.PREC_PRECISE)), k))
+                o = pool[k].new_outputs()[0] if i in own else outs[k]
+                rids.append((submit(k, o), k, o, i in own))
             lat, first, last, units = [], None, None, 0.0
-            for r, k in rids:
+            for r, k, o, mine in rids:
                 rc = srv.wait(r)
                 if rc != 0:
                     raise RuntimeError("request failed: %d %s" % (rc, sb.last_error()))
@@ -661,6 +732,8 @@ def run_serve(args, rank, world, local_rank):
                 last = td if last is None else max(last, td)
                 units += pool[k].units
                 srv.release(r)
+                if mine:
+                    picks.append((k, o))
             lat = np.array(lat)
             sweep.append({"rate_req_s": rate, "requests": nreq,
                           "achieved_rate_req_s": nreq / (arrive[-1] if arrive[-1] > 0 else 1.0),
@@ -668,23 +741,66 @@ def run_serve(args, rank, world, local_rank):
                           "mean_ms": float(lat.mean()),
                           "throughput_gpix_pulses_s": units / (last - first) / 1e9,
                           "batches": srv.stats()["batches"] - b0})
-        clk = clocks.stop() if clocks else {}
+        clk = clocks.stop()
         peak = srv.stats()["peak_bytes"]
+        c1 = srv.counters()
     finally:
         srv.close()
+    t0 = time.time()
+    errs = fp64_sample_rel_l2(pool, picks, seed)
+    nall = nreq * len(rates)
+    return {"sweep": sweep, "peak_device_bytes": peak, "clocks": clk, "synthesis_seconds": synth_s,
+            "lanes": lanes,
+            "residency": {
+                "registered_apertures": len(pool) if resident else 0, "register_seconds": reg_s,
+                "h2d_bytes_per_request": (c1["h2d_bytes"] - c0["h2d_bytes"]) / nall,
+                "phase_history_bytes_per_request_if_uploaded": float(np.mean(
+                    [pool[k].phs.nbytes + pool[k].k64.nbytes + pool[k].p64.nbytes + pool[k].k32.nbytes
+                     + pool[k].p32.nbytes for k in range(len(pool))])),
+                "range_compressed_pulses_during_sweep": c1["rc_pulses"] - c0["rc_pulses"],
+                "requests_served_from_resident_apertures": c1["resident_requests"] - c0["resident_requests"]},
+            "fp64_sample": {"requests": len(errs), "of": nreq * len(rates), "pixels_per_image": 1000,
+                            "rel_l2_max": max(errs), "rel_l2_median": float(np.median(errs)),
+                            "target": 1e-3, "oracle_seconds": time.time() - t0},
+            "latency": "submission to complex image in pinned host memory",
+            "workload": "%d requests per rate drawn from 96 uneven jobs (batch96 distribution), rates %s "
+                        "req/s, %d lanes, batches <= 32, HBM budget 150 GB, PREC_PRECISE, %s"
+                        % (nreq, "/".join("%g" % r for r in rates), lanes,
+                           "phase histories registered once (resident range profiles)" if resident
+                           else "each request uploads and range-compresses its phase history")}
+
+
+def run_serve(args, rank, world, local_rank):
+    """--config serve: the serving sweep on its own (see serve_measure)."""
+    import torch
+    import sarbp_b200 as sb
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    ctx = sb.Context(local_rank)
+    rates = [float(x) for x in args.serve_rates.split(",")]
+    try:
+        s = serve_measure(torch, ctx, dev, rates, args.serve_requests, args.serve_lanes, args.serve_batch_work,
+                          7 + rank)
+        # the same top rate with every request uploading and range-compressing
+        # its own phase history, for comparison
+        u = serve_measure(torch, ctx, dev, rates[-1:], args.serve_requests, args.serve_lanes,
+                          args.serve_batch_work, 7 + rank, resident=False)
+    finally:
         ctx.close()
-    top = sweep[-1]
+    top = s["sweep"][-1]
     out = {
         "metric": "serving p99 latency at %g req/s (ms)" % top["rate_req_s"],
-        "value": top["p99_ms"], "unit": "ms", "n_gpus": world, "steps": nreq, "warmup": len(pool),
-        "ms_per_step": top["mean_ms"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 (split-precision; f64 per-pulse set-up, PREC_PRECISE)",
+        "value": top["p99_ms"], "unit": "ms", "n_gpus": world, "steps": args.serve_requests,
+        "warmup": 96, "ms_per_step": top["mean_ms"], "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (split-precision; f64 per-pulse set-up, PREC_PRECISE)",
         "data": "synthetic (seeded uneven jobs, Poisson arrivals)",
-        "config": {"workload": "serve: %d requests per rate drawn from 96 uneven jobs (batch96 distribution), "
-                               "rates %s req/s, %d lanes, batches <= 32, HBM budget 150 GB"
-                               % (nreq, args.serve_rates, args.serve_lanes),
-                   "parallelism": "replicas%d" % world, "latency": "submission to complex image in pinned host memory"},
-        "sweep": sweep, "peak_device_bytes": peak, "clocks": clk, "synthesis_seconds": synth_s,
+        "config": {"workload": "serve: " + s["workload"], "parallelism": "replicas%d" % world,
+                   "latency": s["latency"]},
+        "sweep": s["sweep"], "fp64_sample": s["fp64_sample"], "residency": s["residency"],
+        "peak_device_bytes": s["peak_device_bytes"],
+        "uploading_each_request": {"sweep": u["sweep"], "residency": u["residency"]},
+        "clocks": s["clocks"], "synthesis_seconds": s["synthesis_seconds"],
     }
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -430,6 +430,25 @@ int sarbp_img_output_u8_device(sarbp_ctx *ctx, const double *dB, int nu, int nv,
     return SARBP_OK;
 }
 
+int sarbp_img_output_u8_from_img_device(sarbp_ctx *ctx, const double *img, int nu, int nv,
+                                        double dB_min, double dB_max, uint8_t *out) {
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    if (!img || !out || nu < 1 || nv < 1) return fail(SARBP_ERR_INVALID, "bad u8 arguments");
+    if (!(dB_min < dB_max)) return fail(SARBP_ERR_INVALID, "Constraint failed: dB_min < dB_max");
+    cudaError_t e = ctx->out_aux.ensure(256, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "allocating");
+    auto *m = static_cast<unsigned long long *>(ctx->out_aux.ptr);
+    const long long n = (long long)nu * nv;
+    e = cudaMemsetAsync(m, 0, sizeof(unsigned long long), ctx->stream);
+    if (e == cudaSuccess) e = launch_maxabs(reinterpret_cast<const double2 *>(img), n, m, ctx->stream);
+    if (e == cudaSuccess)
+        e = launch_img_u8(reinterpret_cast<const double2 *>(img), n, m, out, dB_min, dB_max, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "u8 launch");
+    ctx->dev.launches += 2;
+    return SARBP_OK;
+}
+
 int sarbp_img_output_to_dB(sarbp_ctx *ctx, const double *img, int nu, int nv, double *dB) {
     int rc = set_device(ctx);
     if (rc) return rc;
@@ -474,6 +493,14 @@ int sarbp_taylor(int num, double S_L, double *out) {
     if (num < 2 || !out) return fail(SARBP_ERR_INVALID, "taylor: num >= 2 and out required");
     if (!(S_L >= 1.0)) return fail(SARBP_ERR_INVALID, "taylor: S_L >= 1 required");
     taylor_window(num, S_L, out);
+    return SARBP_OK;
+}
+
+int sarbp_taylor_mode(int num, double S_L, int mode, double *out) {
+    if (mode != SARBP_TAYLOR_REF && mode != SARBP_TAYLOR_FLOAT) return fail(SARBP_ERR_INVALID, "taylor: unknown mode");
+    if (num < 2 || !out) return fail(SARBP_ERR_INVALID, "taylor: num >= 2 and out required");
+    if (!(S_L >= 1.0)) return fail(SARBP_ERR_INVALID, "taylor: S_L >= 1 required");
+    taylor_window(num, S_L, out, mode);
     return SARBP_OK;
 }
 

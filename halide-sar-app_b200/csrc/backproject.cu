@@ -484,8 +484,22 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
                 bar_arrive(kBarEmpty0 + b);
             }
         }
-        // ---- final phase, row flip (backprojection.cpp:130-138), max|z| ----
+        // ---- final phase, row flip (backprojection.cpp:130-138), max|z|;
+        // a pulse chunk adds its sums to the partial image instead ----
         double zmax = 0.0;
+        if (jb.acc) {
+#pragma unroll
+            for (int k = 0; k < PPT; ++k) {
+                int ix, iy;
+                pixel_of(ti.transposed != 0, tx0, ty0, k, ix, iy);
+                if (ix < nu && iy < nv) {
+                    float2 *a = jb.acc + (long long)iy * nu + ix;
+                    const float2 s = *a;
+                    *a = make_float2(s.x + ((k & 1) ? arp[k >> 1].y : arp[k >> 1].x),
+                                     s.y + ((k & 1) ? aip[k >> 1].y : aip[k >> 1].x));
+                }
+            }
+        } else
 #pragma unroll
         for (int k = 0; k < PPT; ++k) {
             int ix, iy;
@@ -503,7 +517,7 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
         zmax = warp_max(zmax);
         if (lane == 0) sm.sred[warp] = zmax;
         __syncthreads();
-        if (tid == 0) {
+        if (tid == 0 && !jb.acc) {
             double m = 0.0;
             for (int w = 0; w < kConsumerWarps; ++w) m = fmax(m, sm.sred[w]);
             atomicMax(&jb.sc->maxabs, (unsigned long long)__double_as_longlong(m));

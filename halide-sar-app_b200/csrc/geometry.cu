@@ -124,7 +124,7 @@ __device__ __forceinline__ double warp_max_d(double v) {
 // between the two passes; up to 4 the registers fit three CTAs per SM.
 template <int GP>
 __global__ void __launch_bounds__(kThreadsGeom, GP <= 4 ? 3 : 2)
-    tile_setup_kernel(const DevJob *__restrict__ jobs, const WorkItem *__restrict__ items) {
+    tile_setup_kernel(const DevJob *__restrict__ jobs, const WorkItem *__restrict__ items, int records) {
     constexpr int kWarps = kThreadsGeom / 32;
     __shared__ double sbox[kWarps][6];
     __shared__ float srho[kWarps];
@@ -281,6 +281,7 @@ __global__ void __launch_bounds__(kThreadsGeom, GP <= 4 ? 3 : 2)
         if (bad) atomicOr(&jb.sc->status, kStatusNonFinite);
     }
     __syncthreads();
+    if (!records) return;  // pulse-chunked jobs form their records per chunk
     // ---- this tile's pulse records ----
     const TileInfo t = s_tile;
     bool bad_pulse = false;
@@ -297,18 +298,46 @@ __global__ void __launch_bounds__(kThreadsGeom, GP <= 4 ? 3 : 2)
     if (__any_sync(0xffffffffu, bad_pulse) && lane == 0) atomicOr(&jb.sc->status, kStatusNonFinite);
 }
 
+// Records only, for the pulses of one chunk of a pulse-chunked job: the
+// tile table was formed ahead of the first chunk (tile_setup_kernel with
+// records = 0), jb.P is the chunk's pulse count and jb.pulse its pulse table.
+__global__ void __launch_bounds__(kThreadsGeom)
+    tile_records_kernel(const DevJob *__restrict__ jobs, const WorkItem *__restrict__ items) {
+    const WorkItem wi = items[blockIdx.x];
+    const DevJob &jb = jobs[wi.job];
+    const TileInfo t = jb.tiles[wi.tile];
+    RecConst rk;
+    rk.k_c = jb.sc->k_c;
+    rk.half_inv_kc = 0.5 / rk.k_c;
+    rk.ilk = jb.inv_lsr / rk.k_c;
+    PulseRec *recs = jb.recs + (size_t)wi.tile * jb.P;
+    bool bad_pulse = false;
+    for (int p = threadIdx.x; p < jb.P; p += kThreadsGeom) {
+        PulseRec rec;
+        bad_pulse |= !make_record(jb, t, rk, p, rec);
+        recs[p] = rec;
+    }
+    if (__any_sync(0xffffffffu, bad_pulse) && (threadIdx.x & 31) == 0) atomicOr(&jb.sc->status, kStatusNonFinite);
+}
+
 }  // namespace
 
 cudaError_t launch_tile_setup(const DevJob *d_jobs, const WorkItem *d_items, int nitems, int tile_pixels,
-                              cudaStream_t st) {
+                              cudaStream_t st, int records) {
     if (nitems <= 0) return cudaSuccess;
     if (tile_pixels < 1 || tile_pixels > 8 * kThreadsGeom) return cudaErrorInvalidValue;
     if (tile_pixels <= 2 * kThreadsGeom)
-        tile_setup_kernel<2><<<nitems, kThreadsGeom, 0, st>>>(d_jobs, d_items);
+        tile_setup_kernel<2><<<nitems, kThreadsGeom, 0, st>>>(d_jobs, d_items, records);
     else if (tile_pixels <= 4 * kThreadsGeom)
-        tile_setup_kernel<4><<<nitems, kThreadsGeom, 0, st>>>(d_jobs, d_items);
+        tile_setup_kernel<4><<<nitems, kThreadsGeom, 0, st>>>(d_jobs, d_items, records);
     else
-        tile_setup_kernel<8><<<nitems, kThreadsGeom, 0, st>>>(d_jobs, d_items);
+        tile_setup_kernel<8><<<nitems, kThreadsGeom, 0, st>>>(d_jobs, d_items, records);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tile_records(const DevJob *d_jobs, const WorkItem *d_items, int nitems, cudaStream_t st) {
+    if (nitems <= 0) return cudaSuccess;
+    tile_records_kernel<<<nitems, kThreadsGeom, 0, st>>>(d_jobs, d_items);
     return cudaGetLastError();
 }
 

@@ -4,6 +4,8 @@
 
 #include <cmath>
 
+#include "sarbp_b200.h"
+
 namespace sarbp {
 
 namespace {
@@ -21,8 +23,12 @@ long long div_floor(long long a, long long b) {
 // to f32 (pow and acosh then run in f32); pow(e, 2) with a constant integer
 // exponent is a square in e's own type, so the F_m denominator term
 // pow(m+1, 2) / pow(r+1, 2) is an Int32 division; the f32 sign
-// pow(-1, m+2) multiplies the numerator once per r.
-std::vector<double> taylor_coefficients(double S_L) {
+// pow(-1, m+2) multiplies the numerator once per r.  With
+// SARBP_TAYLOR_FLOAT the denominator term is a floating-point quotient
+// (the published RITSAR window, which the Halide expression restates);
+// everything else is the same.  Writes min(count, cap) coefficients into
+// out and returns count = n_bar - 1; allocates nothing.
+int taylor_coefficients_into(double S_L, double *out, int cap, int mode) {
     const float p10 = std::pow(10.0f, (float)(S_L * (1.0 / 20)));
     const float acosh_f = std::log(p10 + std::sqrt(p10 * p10 - 1.0f));
     const double A = (1.0 / kPi) * (double)acosh_f;
@@ -32,8 +38,7 @@ std::vector<double> taylor_coefficients(double S_L) {
     const double sigma_p = (double)n_bar / std::sqrt(A2 + nh * nh);
     const double sp2 = sigma_p * sigma_p;
     const int nr = n_bar - 1;
-    std::vector<double> F(nr > 0 ? nr : 0);
-    for (int m = 0; m < nr; ++m) {
+    for (int m = 0; m < nr && m < cap; ++m) {
         const long long m1sq = (long long)(m + 1) * (m + 1);
         const float sgn = std::pow(-1.0f, (float)(m + 2));
         double num = 1.0, den = 1.0;
@@ -42,41 +47,26 @@ std::vector<double> taylor_coefficients(double S_L) {
             num = num * ((double)sgn * (1.0 - (double)m1sq / sp2 / (A2 + rh * rh)));
             if (r != m) {
                 const long long r1sq = (long long)(r + 1) * (r + 1);
-                den = den * (1.0 - (double)div_floor(m1sq, r1sq));
+                const double q = mode == SARBP_TAYLOR_FLOAT ? (double)m1sq / (double)r1sq
+                                                            : (double)div_floor(m1sq, r1sq);
+                den = den * (1.0 - q);
             }
-        }
-        F[m] = num / den;
-    }
-    return F;
-}
-
-// signal.h:28-41 as above, for callers that may not allocate.
-int taylor_coefficients_into(double S_L, double *out, int cap) {
-    const float p10 = std::pow(10.0f, (float)(S_L * (1.0 / 20)));
-    const float acosh_f = std::log(p10 + std::sqrt(p10 * p10 - 1.0f));
-    const double A = (1.0 / kPi) * (double)acosh_f;
-    const double A2 = A * A;
-    const int n_bar = (int)(2 * A2 + 0.5) + 1;
-    const double nh = (double)n_bar - 0.5;
-    const double sp2 = ((double)n_bar / std::sqrt(A2 + nh * nh)) * ((double)n_bar / std::sqrt(A2 + nh * nh));
-    const int nr = n_bar - 1;
-    for (int m = 0; m < nr && m < cap; ++m) {
-        const long long m1sq = (long long)(m + 1) * (m + 1);
-        const float sgn = std::pow(-1.0f, (float)(m + 2));
-        double num = 1.0, den = 1.0;
-        for (int r = 0; r < nr; ++r) {
-            const double rh = (double)r + 0.5;
-            num = num * ((double)sgn * (1.0 - (double)m1sq / sp2 / (A2 + rh * rh)));
-            if (r != m) den = den * (1.0 - (double)div_floor(m1sq, (long long)(r + 1) * (r + 1)));
         }
         out[m] = num / den;
     }
     return nr > 0 ? nr : 0;
 }
 
+std::vector<double> taylor_coefficients(double S_L, int mode) {
+    const int n = taylor_coefficients_into(S_L, nullptr, 0, mode);
+    std::vector<double> F(n);
+    taylor_coefficients_into(S_L, F.data(), n, mode);
+    return F;
+}
+
 // signal.h:43-48: w(x) = 1 + sum_r F(r) cos(2 pi (r+1) xi), xi = linspace(-1/2, 1/2, num)
-void taylor_window(int num, double S_L, double *out) {
-    const std::vector<double> F = taylor_coefficients(S_L);
+void taylor_window(int num, double S_L, double *out, int mode) {
+    const std::vector<double> F = taylor_coefficients(S_L, mode);
     const double step = (0.5 - (-0.5)) / (double)(num - 1);
     double wmax = -INFINITY;
     for (int x = 0; x < num; ++x) {

@@ -6,13 +6,14 @@
 namespace sarbp {
 
 // Taylor window coefficients F_m (signal.h:28-41) for side-lobe level S_L;
-// returns n_bar - 1 values.
-std::vector<double> taylor_coefficients(double S_L);
+// returns n_bar - 1 values.  mode: SARBP_TAYLOR_REF (the reference's Int32
+// division in the F_m denominator) or SARBP_TAYLOR_FLOAT (a float quotient).
+std::vector<double> taylor_coefficients(double S_L, int mode = 0);
 // The same coefficients written into out[0..cap) without allocating; returns
 // their count (n_bar - 1), which may exceed cap (then only cap are written).
-int taylor_coefficients_into(double S_L, double *out, int cap);
+int taylor_coefficients_into(double S_L, double *out, int cap, int mode = 0);
 // Full Taylor window (signal.h:14-51), normalised to its maximum.
-void taylor_window(int num, double S_L, double *out);
+void taylor_window(int num, double S_L, double *out, int mode = 0);
 
 // ImgPlane.cpp:20-28 / ip.h:5-9
 int ip_upsample(int n);

@@ -93,6 +93,12 @@ struct DevJob {
     double2 *out;         // [nv][nu]
     uint8_t *out_u8;      // [nv][nu] or null
     double dB_min, dB_max;
+    // pulse-chunked jobs: the descriptor of one chunk has P = the chunk's
+    // pulses, phs its phase-history rows in order (no fftshift rotation:
+    // wP and pulse are the chunk's gathered window and pulse table), and
+    // the backprojection adds its sums into acc instead of writing out
+    int chunked;
+    float2 *acc;          // [nv][nu] partial image (pixel-row order) or null
 };
 
 // (job, tile) work item of the per-tile kernels

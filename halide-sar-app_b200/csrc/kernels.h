@@ -40,9 +40,19 @@ cudaError_t launch_backproject(const BpLaunch &L, const DevJob *d_jobs, const Wo
 cudaError_t launch_backproject_naive(const DevJob *d_jobs, int job, int nu, int nv, cudaStream_t st);
 
 // geometry.cu
+// records = 0: tile table and final phases only (pulse-chunked jobs)
 cudaError_t launch_tile_setup(const DevJob *d_jobs, const WorkItem *d_items, int nitems, int tile_pixels,
-                              cudaStream_t st);
+                              cudaStream_t st, int records = 1);
+// per-(tile, pulse) records of one pulse chunk over an existing tile table
+cudaError_t launch_tile_records(const DevJob *d_jobs, const WorkItem *d_items, int nitems, cudaStream_t st);
 
+
+// accum_kernels.cu (pulse-chunked jobs)
+cudaError_t launch_store_job(const DevJob &dj, DevJob *d_dst, cudaStream_t st);
+cudaError_t launch_chunk_tables(const double4 *pulse, const float *wP, int P, int q0, int n, double4 *pulse_c,
+                                float *wP_c, cudaStream_t st);
+cudaError_t launch_finalize(const DevJob *d_job, long long npix, int num_sms, cudaStream_t st);
+cudaError_t launch_fill_items(WorkItem *items, int ntiles, RowItem *rows, int nrows, cudaStream_t st);
 
 // peaks.cu
 cudaError_t measure_peaks(int num_sms, cudaStream_t st, double *ffma_per_s, double *mufu_per_s);
@@ -53,6 +63,9 @@ cudaError_t launch_db_u8(const double2 *img, long long n, const unsigned long lo
                          double *dB, uint8_t *u8, double dB_min, double dB_max, cudaStream_t st);
 cudaError_t launch_u8_from_db(const double *dB, long long n, double dB_min, double dB_max,
                               uint8_t *u8, cudaStream_t st);
+// u8 image straight from a complex image and its max|z| (no f64 dB image)
+cudaError_t launch_img_u8(const double2 *img, long long n, const unsigned long long *d_max, uint8_t *u8,
+                          double lo, double hi, cudaStream_t st);
 // u8 images of every job of a batch that asked for one (uses DevJob::maxabs)
 cudaError_t launch_batch_u8(const DevJob *d_jobs, int njobs, long long max_pixels, cudaStream_t st);
 

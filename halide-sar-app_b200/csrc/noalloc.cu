@@ -1,14 +1,17 @@
 // noalloc.cu -- backprojection of one job without any memory allocation.
 //
-// Some callers cannot allocate device memory at the time they want an image:
-// code running inside a CUDA stream capture, hosts whose device memory is
-// handed out up front by a pool or an allocator they do not own, or
-// real-time loops that must not hit the allocator.  For them this file gives
-// one more entry point, sarbp_backprojection_noalloc, that runs the same
-// kernels as sarbp_backprojection_device but keeps every scratch array
-// (range-profile pairs, windows, pulse table, tile table, per-(tile, pulse)
-// records, final phases, descriptors, work list, twiddles) in one
-// file-scope device array of kScratchBytes.  No context is created and
+// Some callers must not allocate device memory at the time they want an
+// image: processes whose device memory is handed out up front by a pool or
+// an allocator they do not own (a cudaMalloc there fails, or fragments and
+// bypasses the pool), and real-time loops that cannot take cudaMalloc's
+// latency and its implicit device synchronisation on the path that forms
+// each image.  For them this file gives one more entry point,
+// sarbp_backprojection_noalloc, that runs the same kernels as
+// sarbp_backprojection_device but keeps every scratch array (range-profile
+// pairs, windows, pulse table, tile table, per-(tile, pulse) records, final
+// phases, descriptors, work list) in one file-scope device array of
+// kScratchBytes, whose first kTwiddleBytes hold the FFT twiddle tables of
+// every supported N_fft, filled once per device.  No context is created and
 // nothing is allocated, on the device or on the host.
 //
 // Consequences a caller must know:
@@ -17,8 +20,12 @@
 //  - a job whose scratch exceeds the array is rejected (SARBP_ERR_UNSUPPORTED);
 //  - all calls share the array: calls that overlap on the GPU (two streams,
 //    or two host threads) race and corrupt each other -- serialise them;
-//  - the first call on a device looks up the array's device address and
-//    sets kernel attributes; make that first call before any stream capture.
+//  - the first call on a device looks up the array's device address, sets
+//    kernel attributes and fills the twiddle tables (then waits for its
+//    stream); make that first call before any stream capture;
+//  - the per-device set-up is kept for the life of the process: after a
+//    cudaDeviceReset (or any teardown of the primary context) the cached
+//    address is stale, so the entry point must not be used again.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -39,6 +46,22 @@ namespace {
 constexpr size_t kScratchBytes = size_t(64) << 20;  // 64 MiB
 constexpr int kMaxDevices = 64;
 
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Fixed offsets of the twiddle tables of logN = kMinLogN..kMaxLogN at the
+// start of the scratch (256-byte aligned each).
+constexpr size_t twiddle_offset(int logN) {
+    size_t o = 0;
+    for (int l = kMinLogN; l < logN; ++l) {
+        const int N = 1 << l, R0 = 1 << (l % 4);
+        size_t n = 0;
+        for (int ns = R0 > 1 ? R0 : 16; ns < N; ns *= 16) n += 15 * (size_t)ns;
+        o = (o + (n + 1) * 8 + 255) / 256 * 256;  // float2 entries
+    }
+    return o;
+}
+constexpr size_t kTwiddleBytes = twiddle_offset(kMaxLogN + 1);
+
 // The scratch.  Host code must not use this symbol as an address: the device
 // address comes from cudaGetSymbolAddress below.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
@@ -47,10 +70,26 @@ std::mutex g_setup_mutex;
 void *g_scratch_addr[kMaxDevices] = {};
 int g_num_sms[kMaxDevices] = {};
 
-size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+// Twiddle table of one N (same layout as fill_twiddle_table): for each pass
+// with NS > 1, exp(-2 pi i jm r / (NS 16)) at [(r-1) NS + jm].
+__global__ void twiddle_kernel(float2 *tw, int logN) {
+    const int N = 1 << logN;
+    const int R0 = 1 << (logN % 4);
+    int ns = R0 > 1 ? R0 : 16, off = 0;
+    while (ns < N) {
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < 15 * ns; k += gridDim.x * blockDim.x) {
+            const int r = k / ns + 1, jm = k % ns;
+            const double a = -2.0 * 3.14159265358979323846 * (double)((long long)jm * r) / (double)(ns * 16);
+            tw[off + k] = make_float2((float)cos(a), (float)sin(a));
+        }
+        off += 15 * ns;
+        ns *= 16;
+    }
+}
 
-// Looks up the scratch address on the current device (once per device).
-int scratch_for_device(int dev, void **addr, int *num_sms) {
+// Looks up the scratch address on the current device and fills the twiddle
+// tables (once per device, on `st`, waiting for it).
+int scratch_for_device(int dev, cudaStream_t st, void **addr, int *num_sms) {
     if (dev < 0 || dev >= kMaxDevices) return fail(SARBP_ERR_UNSUPPORTED, "device index too large");
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     if (!g_scratch_addr[dev]) {
@@ -63,6 +102,12 @@ int scratch_for_device(int dev, void **addr, int *num_sms) {
         e = init_range_compress_attributes();
         if (e == cudaSuccess) e = init_backproject_attributes();
         if (e != cudaSuccess) return cuda_fail(e, "setting kernel attributes");
+        for (int l = kMinLogN; l <= kMaxLogN; ++l)
+            twiddle_kernel<<<64, 256, 0, st>>>(reinterpret_cast<float2 *>(static_cast<char *>(p) +
+                                                                          twiddle_offset(l)), l);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, "no-alloc: filling the twiddle tables");
         g_num_sms[dev] = sms;
         g_scratch_addr[dev] = p;
     }
@@ -80,23 +125,6 @@ __global__ void init_items_kernel(WorkItem *items, int ntiles, RowItem *rows, in
     if (t < ntiles) items[t] = WorkItem{0, t};
     if (t < npulses) rows[t] = RowItem{0, t};
     if (t == 0) *counter = 0;
-}
-
-// Twiddle table of one N (same layout as fill_twiddle_table): for each pass
-// with NS > 1, exp(-2 pi i jm r / (NS 16)) at [(r-1) NS + jm].
-__global__ void twiddle_kernel(float2 *tw, int logN) {
-    const int N = 1 << logN;
-    const int R0 = 1 << (logN % 4);
-    int ns = R0 > 1 ? R0 : 16, off = 0;
-    while (ns < N) {
-        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < 15 * ns; k += gridDim.x * blockDim.x) {
-            const int r = k / ns + 1, jm = k % ns;
-            const double a = -2.0 * 3.14159265358979323846 * (double)((long long)jm * r) / (double)(ns * 16);
-            tw[off + k] = make_float2((float)cos(a), (float)sin(a));
-        }
-        off += 15 * ns;
-        ns *= 16;
-    }
 }
 
 __global__ void status_kernel(const JobScalars *sc, int *status) { *status = sc->status; }
@@ -126,10 +154,12 @@ extern "C" int sarbp_backprojection_noalloc(const sarbp_job *job, void *cuda_str
     if (j.out_u8 && !(j.dB_min < j.dB_max)) return bad("dB_min < dB_max is required for the u8 image");
     DevJob dj;
     std::memset(&dj, 0, sizeof(dj));
-    dj.n_taylor = taylor_coefficients_into(j.taylor_s_l, dj.taylor_F, kMaxTaylorTerms);
+    if (j.taylor_mode != SARBP_TAYLOR_REF && j.taylor_mode != SARBP_TAYLOR_FLOAT) return bad("unknown taylor_mode");
+    dj.n_taylor = taylor_coefficients_into(j.taylor_s_l, dj.taylor_F, kMaxTaylorTerms, j.taylor_mode);
     if (dj.n_taylor > kMaxTaylorTerms) return bad("taylor side-lobe level too large");
     for (int k = 0; k < dj.n_taylor; ++k)
-        if (!std::isfinite(dj.taylor_F[k])) return bad("taylor levels above 30 dB have no defined window");
+        if (!std::isfinite(dj.taylor_F[k]))
+            return bad("taylor levels above 30 dB have no defined window (use SARBP_TAYLOR_FLOAT)");
     const double lsa = std::floor((double)(-j.nsamples) * j.delta_r / 2);
     const double lsb = std::floor((double)j.nsamples * j.delta_r / 2);
     if (!(lsb > lsa)) return bad("range axis is empty");
@@ -141,13 +171,12 @@ extern "C" int sarbp_backprojection_noalloc(const sarbp_job *job, void *cuda_str
     const size_t ntiles = (size_t)tiles_x * tiles_y;
     int logN = 0;
     while ((1 << logN) < j.n_fft) ++logN;
-    size_t o = 0;
+    size_t o = kTwiddleBytes;  // the twiddle tables come first
     const size_t o_sc = o;    o = align_up(o + sizeof(JobScalars), 256);
     const size_t o_job = o;   o = align_up(o + sizeof(DevJob), 256);
     const size_t o_items = o; o = align_up(o + ntiles * sizeof(WorkItem), 256);
     const size_t o_rows = o;  o = align_up(o + P * sizeof(RowItem), 256);
     const size_t o_cnt = o;   o = align_up(o + sizeof(int), 256);
-    const size_t o_tw = o;    o = align_up(o + (size_t)(twiddle_table_size(logN) + 1) * sizeof(float2), 256);
     const size_t o_qp = o;    o = align_up(o + P * (N + 1) * sizeof(float4), 256);
     const size_t o_filt = o;  o = align_up(o + S * sizeof(float), 256);
     const size_t o_ws = o;    o = align_up(o + S * sizeof(float), 256);
@@ -166,10 +195,10 @@ extern "C" int sarbp_backprojection_noalloc(const sarbp_job *job, void *cuda_str
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     void *base = nullptr;
     int num_sms = 0;
-    int rc = scratch_for_device(dev, &base, &num_sms);
+    cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+    int rc = scratch_for_device(dev, st, &base, &num_sms);
     if (rc) return rc;
     char *sb = static_cast<char *>(base);
-    cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
 
     // ---- descriptor ----
     dj.S = j.nsamples;
@@ -217,7 +246,7 @@ extern "C" int sarbp_backprojection_noalloc(const sarbp_job *job, void *cuda_str
     DevJob *d_job = reinterpret_cast<DevJob *>(sb + o_job);
     WorkItem *d_items = reinterpret_cast<WorkItem *>(sb + o_items);
     int *d_cnt = reinterpret_cast<int *>(sb + o_cnt);
-    float2 *d_tw = reinterpret_cast<float2 *>(sb + o_tw);
+    const float2 *d_tw = reinterpret_cast<const float2 *>(sb + twiddle_offset(logN));
     RowItem *d_rows = reinterpret_cast<RowItem *>(sb + o_rows);
 
     // ---- launches (the prep kernel clears the job's scalars) ----
@@ -225,7 +254,6 @@ extern "C" int sarbp_backprojection_noalloc(const sarbp_job *job, void *cuda_str
     const size_t nfill = ntiles > P ? ntiles : P;
     init_items_kernel<<<(int)((nfill + 255) / 256), 256, 0, st>>>(d_items, (int)ntiles, d_rows, j.npulses,
                                                                   d_cnt);
-    twiddle_kernel<<<64, 256, 0, st>>>(d_tw, logN);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "no-alloc set-up launches");
     launch_prep(d_job, 1, st);

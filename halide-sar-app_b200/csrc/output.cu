@@ -104,9 +104,23 @@ __global__ void u8_from_db_kernel(const double *__restrict__ dB, long long n, do
         u8[i] = to_u8(dB[i], lo, hi);
 }
 
+// u8 of the four neighbouring pixels [i0, i0 + 4) of an image of n pixels:
+// 64 B of complex f64 in, one 32-bit word of u8 out when the destination is
+// 4-byte aligned (vec).
+__device__ __forceinline__ void u8_quad(const double2 *__restrict__ img, long long n, long long i0,
+                                        uint8_t *__restrict__ u8, bool vec, const U8Scale &us) {
+    if (vec && i0 + 4 <= n) {
+        uint32_t w = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) w |= (uint32_t)u8_of(img[i0 + k], us) << (8 * k);
+        *reinterpret_cast<uint32_t *>(u8 + i0) = w;
+    } else {
+        for (long long i = i0; i < n && i < i0 + 4; ++i) u8[i] = u8_of(img[i], us);
+    }
+}
+
 // blockIdx.y = job; jobs without an u8 output return at once.  Each thread
-// converts four neighbouring pixels (64 B of complex f64 in, one 32-bit word
-// of u8 out when the destination is 4-byte aligned).
+// converts four neighbouring pixels at a time.
 __global__ void batch_u8_kernel(const DevJob *__restrict__ jobs) {
     const DevJob &jb = jobs[blockIdx.y];
     if (!jb.out_u8) return;
@@ -115,17 +129,20 @@ __global__ void batch_u8_kernel(const DevJob *__restrict__ jobs) {
     const U8Scale us = u8_scale(m, jb.dB_min, jb.dB_max);
     const bool vec = ((reinterpret_cast<uintptr_t>(jb.out_u8) & 3) == 0);
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; 4 * q < n; q += stride) {
-        const long long i0 = 4 * q;
-        if (vec && i0 + 4 <= n) {
-            uint32_t w = 0;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) w |= (uint32_t)u8_of(jb.out[i0 + k], us) << (8 * k);
-            *reinterpret_cast<uint32_t *>(jb.out_u8 + i0) = w;
-        } else {
-            for (long long i = i0; i < n && i < i0 + 4; ++i) jb.out_u8[i] = u8_of(jb.out[i], us);
-        }
-    }
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; 4 * q < n; q += stride)
+        u8_quad(jb.out, n, 4 * q, jb.out_u8, vec, us);
+}
+
+// The same conversion for one image given by its pointer and a max|z| from
+// maxabs_kernel.
+__global__ void img_u8_kernel(const double2 *__restrict__ img, long long n,
+                              const unsigned long long *__restrict__ maxbits, uint8_t *__restrict__ u8,
+                              double lo, double hi) {
+    const U8Scale us = u8_scale(__longlong_as_double((long long)*maxbits), lo, hi);
+    const bool vec = ((reinterpret_cast<uintptr_t>(u8) & 3) == 0);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; 4 * q < n; q += stride)
+        u8_quad(img, n, 4 * q, u8, vec, us);
 }
 
 int grid_for(long long n) {
@@ -151,6 +168,14 @@ cudaError_t launch_db_u8(const double2 *img, long long n, const unsigned long lo
 cudaError_t launch_u8_from_db(const double *dB, long long n, double lo, double hi, uint8_t *u8,
                               cudaStream_t st) {
     u8_from_db_kernel<<<grid_for(n), 256, 0, st>>>(dB, n, lo, hi, u8);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_img_u8(const double2 *img, long long n, const unsigned long long *d_max, uint8_t *u8,
+                          double lo, double hi, cudaStream_t st) {
+    // about eight 256-thread blocks per SM, four pixels per thread
+    const long long bx = std::max<long long>(1, std::min<long long>((n / 4 + 255) / 256, 148LL * 8));
+    img_u8_kernel<<<(unsigned)bx, 256, 0, st>>>(img, n, d_max, u8, lo, hi);
     return cudaGetLastError();
 }
 

@@ -3,7 +3,9 @@
 // Replaces backprojection.cpp:79-104 and the FFTW extern (dft.cpp:40-79):
 // for each output pulse row p of each job
 //   src     = (p + 2*ceil(P/2)) mod P     (fftshift over the pulse axis,
-//                                          applied twice: :98 and :104)
+//                                          applied twice: :98 and :104;
+//                                          src = p for a pulse chunk, whose
+//                                          rows come in phase-history order)
 //   x[n]    = phs[src][s] * |k_r[s]| * wS[s] * wP[src],
 //             s = ((n + N/2) mod N) - (N - S)/2, zero outside [0, S)
 //                                         (window, filter, pad, fftshift)
@@ -203,7 +205,7 @@ range_compress_kernel(const DevJob *__restrict__ jobs, const RowItem *__restrict
     const DevJob &jb = jobs[it.job];
     const int S = jb.S, P = jb.P, p = it.pulse;
     const int pm = P / 2 + P % 2;
-    const int src = (int)(((long long)p + 2 * pm) % P);
+    const int src = jb.chunked ? p : (int)(((long long)p + 2 * pm) % P);
     const int x_pad = (N - S) >> 1;  // floor division by 2
     const float2 *__restrict__ ph = jb.phs + (size_t)src * S;
     const float wp = live ? jb.wP[src] : 0.f;

@@ -28,7 +28,8 @@ struct JobLayout {
 // Scratch of one job: profiles (pairs for the tile kernel, plain Q for the
 // range-compression-only entry point), windows, pulse table, and for the
 // tile kernel the tile table, per-(tile, pulse) records and final phases.
-JobLayout layout_of(const sarbp_job &j, size_t base, int tile_x, int tile_y, bool rc_only, bool naive) {
+JobLayout layout_of(const sarbp_job &j, size_t base, int tile_x, int tile_y, bool rc_only, bool naive,
+                    bool resident = false) {
     JobLayout L;
     const size_t P = (size_t)j.npulses, N = (size_t)j.n_fft, S = (size_t)j.nsamples;
     const bool tiles = !rc_only && !naive;
@@ -36,7 +37,7 @@ JobLayout layout_of(const sarbp_job &j, size_t base, int tile_x, int tile_y, boo
         tiles ? (size_t)((j.nu + tile_x - 1) / tile_x) * (size_t)((j.nv + tile_y - 1) / tile_y) : 0;
     size_t o = base;
     L.Q = o;      o = align_up(o + (rc_only ? P * N * sizeof(float2) : 0), 256);
-    L.Qp = o;     o = align_up(o + (rc_only ? 0 : P * (N + 1) * sizeof(float4)), 256);
+    L.Qp = o;     o = align_up(o + (rc_only || resident ? 0 : P * (N + 1) * sizeof(float4)), 256);
     L.filt = o;   o = align_up(o + S * sizeof(float), 256);
     L.wS = o;     o = align_up(o + S * sizeof(float), 256);
     L.wP = o;     o = align_up(o + P * sizeof(float), 256);
@@ -53,7 +54,9 @@ int precision_of(const sarbp_job &j, const sarbp_opts *o) {
     return o ? o->precision : SARBP_PREC_COMPAT;
 }
 
-int validate(const sarbp_job &j, int prec, int idx, bool rc_only) {
+}  // namespace
+
+int validate_job(const sarbp_job &j, int prec, int idx, bool rc_only, bool need_phs) {
     auto bad = [&](const std::string &what) {
         return fail(SARBP_ERR_INVALID, "job " + std::to_string(idx) + ": " + what);
     };
@@ -68,25 +71,67 @@ int validate(const sarbp_job &j, int prec, int idx, bool rc_only) {
     if (!(std::isfinite(j.delta_r))) return bad("delta_r must be finite");
     if (prec != SARBP_PREC_COMPAT && prec != SARBP_PREC_PRECISE && prec != SARBP_PREC_NAIVE)
         return bad("unknown precision mode");
-    if (!j.phs) return bad("phs is NULL");
+    if (need_phs && !j.phs) return bad("phs is NULL");
     if (!j.k_r && !(prec == SARBP_PREC_PRECISE && j.k_r64)) return bad("k_r is NULL");
     if (!j.pos && !(prec == SARBP_PREC_PRECISE && j.pos64)) return bad("pos is NULL");
     if (!rc_only && !j.r && !(j.u && j.v)) return bad("pixel positions: r, or u and v, are required");
     if (!rc_only && !j.output_img) return bad("output_img is NULL");
     if (j.out_u8 && !(j.dB_min < j.dB_max)) return bad("dB_min < dB_max is required for the u8 image");
-    const std::vector<double> F = taylor_coefficients(j.taylor_s_l);
+    if (j.taylor_mode != SARBP_TAYLOR_REF && j.taylor_mode != SARBP_TAYLOR_FLOAT)
+        return bad("unknown taylor_mode");
+    const std::vector<double> F = taylor_coefficients(j.taylor_s_l, j.taylor_mode);
     if ((int)F.size() > kMaxTaylorTerms) return bad("taylor side-lobe level too large (n_bar > 65)");
     for (double f : F)
         if (!std::isfinite(f))
             return bad("taylor " + std::to_string(j.taylor_s_l) +
                        " dB: the window formula of signal.h:39-41 divides by zero for side-lobe "
-                       "levels above 30 dB (its F_m denominator uses Int32 division)");
+                       "levels above 30 dB (its F_m denominator uses Int32 division); "
+                       "SARBP_TAYLOR_FLOAT takes that quotient in floating point");
     const double lsa = std::floor((double)(-j.nsamples) * j.delta_r / 2);
     const double lsb = std::floor((double)j.nsamples * j.delta_r / 2);
     if (!(lsb > lsa)) return bad("range axis is empty: floor(S*delta_r/2) <= floor(-S*delta_r/2)");
     return SARBP_OK;
 }
-}  // namespace
+
+void describe_job(const sarbp_job &j, int prec, int tile_x, int tile_y, DevJob &dj) {
+    dj.S = j.nsamples;
+    dj.P = j.npulses;
+    dj.N = j.n_fft;
+    dj.nu = j.nu;
+    dj.nv = j.nv;
+    dj.precision = prec;
+    dj.tile_x = tile_x;
+    dj.tile_y = tile_y;
+    dj.tiles_x = (j.nu + tile_x - 1) / tile_x;
+    dj.tiles_y = (j.nv + tile_y - 1) / tile_y;
+    dj.logN = ilog2i(j.n_fft);
+    dj.n_taylor = taylor_coefficients_into(j.taylor_s_l, dj.taylor_F, kMaxTaylorTerms, j.taylor_mode);
+    dj.phs = reinterpret_cast<const float2 *>(j.phs);
+    dj.k_r32 = j.k_r;
+    dj.k_r64 = j.k_r64;
+    dj.pos32 = j.pos;
+    dj.pos64 = j.pos64;
+    dj.r = j.r;
+    dj.u = j.u;
+    dj.v = j.v;
+    for (int k = 0; k < 3; ++k) {
+        dj.uh[k] = j.u_hat[k];
+        dj.vh[k] = j.v_hat[k];
+    }
+    dj.delta_r = j.delta_r;
+    // backprojection.cpp:120 and :53: lsa = floor(-S*dr/2), lsb = floor(S*dr/2),
+    // lsr = (lsb - lsa) / (N_fft - 1)
+    dj.lsa = std::floor((double)(-j.nsamples) * j.delta_r / 2);
+    const double lsb = std::floor((double)j.nsamples * j.delta_r / 2);
+    dj.lsr = (lsb - dj.lsa) / (double)(j.n_fft - 1);
+    dj.inv_lsr = 1.0 / dj.lsr;
+    dj.out = reinterpret_cast<double2 *>(j.output_img);
+    dj.out_u8 = j.out_u8;
+    dj.dB_min = j.dB_min;
+    dj.dB_max = j.dB_max;
+    dj.chunked = 0;
+    dj.acc = nullptr;
+}
 
 void set_error(const std::string &msg) { g_error = msg; }
 int fail(int code, const std::string &msg) {
@@ -109,6 +154,17 @@ cudaError_t DeviceBuffer::ensure(size_t bytes, cudaStream_t st) {
         cap = 0;
     }
     const size_t want = align_up(bytes + bytes / 8, 1 << 20);
+    cudaError_t e = cudaMalloc(&ptr, want);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        return e;
+    }
+    cap = want;
+    return cudaSuccess;
+}
+cudaError_t DeviceBuffer::alloc_exact(size_t bytes) {
+    release();
+    const size_t want = align_up(bytes > 0 ? bytes : 1, 256);
     cudaError_t e = cudaMalloc(&ptr, want);
     if (e != cudaSuccess) {
         ptr = nullptr;
@@ -210,9 +266,9 @@ BpLaunch default_launch(const sarbp_opts *opts, int num_sms) {
     return L;
 }
 
-size_t Runner::job_scratch_bytes(const sarbp_job &j, const sarbp_opts *opts) {
+size_t Runner::job_scratch_bytes(const sarbp_job &j, const sarbp_opts *opts, bool resident_profiles) {
     const BpLaunch L = default_launch(opts, 148);
-    return layout_of(j, 0, L.tile_x, L.tile_y, false, j.precision == SARBP_PREC_NAIVE).end;
+    return layout_of(j, 0, L.tile_x, L.tile_y, false, j.precision == SARBP_PREC_NAIVE, resident_profiles).end;
 }
 
 Runner::~Runner() {
@@ -231,8 +287,10 @@ void Runner::tile_shape(const sarbp_opts *opts, int *tile_x, int *tile_y) {
 }
 
 int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cudaStream_t st,
-                    void *q_out, bool for_graph, const SlabSpec *slabs) {
+                    void *q_out, bool for_graph, const SlabSpec *slabs, const float4 *const *resident_qp) {
     const bool rc_only = q_out != nullptr;
+    if (rc_only) resident_qp = nullptr;
+    auto resident = [&](int i) { return resident_qp && resident_qp[i]; };
     if (slabs && slabs->nslabs > 0) {
         if (njobs != 1 || rc_only || for_graph || !slabs->row0 || !slabs->aux || !slabs->done)
             return fail(SARBP_ERR_INVALID, "row slabs need one job, a second stream and done events");
@@ -255,7 +313,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
     std::vector<int> prec(njobs);
     for (int i = 0; i < njobs; ++i) {
         prec[i] = precision_of(jobs[i], opts);
-        int rc = validate(jobs[i], prec[i], i, rc_only);
+        int rc = validate_job(jobs[i], prec[i], i, rc_only, !resident(i));
         if (rc) return rc;
     }
     if (!meta_done_) {
@@ -266,7 +324,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
     size_t off = align_up((size_t)njobs * sizeof(JobScalars), 256);
     std::vector<JobLayout> lay(njobs);
     for (int i = 0; i < njobs; ++i) {
-        lay[i] = layout_of(jobs[i], off, L.tile_x, L.tile_y, rc_only, prec[i] == SARBP_PREC_NAIVE);
+        lay[i] = layout_of(jobs[i], off, L.tile_x, L.tile_y, rc_only, prec[i] == SARBP_PREC_NAIVE, resident(i));
         off = lay[i].end;
     }
     if (for_graph && (scratch_.cap < off || pool_ || status_pin_.cap < njobs * sizeof(JobScalars)))
@@ -311,9 +369,10 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
     std::vector<WorkItem> items;
     std::vector<int> naive;
     for (int i = 0; i < njobs; ++i) {
-        const int logN = ilog2i(jobs[i].n_fft);
-        auto &v = rows[logN];
-        for (int p = 0; p < jobs[i].npulses; ++p) v.push_back(RowItem{i, p});
+        if (!resident(i)) {  // resident profiles were range-compressed before
+            auto &v = rows[ilog2i(jobs[i].n_fft)];
+            for (int p = 0; p < jobs[i].npulses; ++p) v.push_back(RowItem{i, p});
+        }
         if (rc_only) continue;
         if (prec[i] == SARBP_PREC_NAIVE) {
             naive.push_back(i);
@@ -352,38 +411,11 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
     for (int i = 0; i < njobs; ++i) {
         const sarbp_job &j = jobs[i];
         DevJob &dj = hj[i];
-        dj.S = j.nsamples;
-        dj.P = j.npulses;
-        dj.N = j.n_fft;
-        dj.nu = j.nu;
-        dj.nv = j.nv;
-        dj.precision = prec[i];
-        dj.tile_x = L.tile_x;
-        dj.tile_y = L.tile_y;
-        dj.tiles_x = (j.nu + L.tile_x - 1) / L.tile_x;
-        dj.tiles_y = (j.nv + L.tile_y - 1) / L.tile_y;
-        dj.logN = ilog2i(j.n_fft);
-        const std::vector<double> F = taylor_coefficients(j.taylor_s_l);
-        dj.n_taylor = (int)F.size();
-        for (size_t k = 0; k < F.size(); ++k) dj.taylor_F[k] = F[k];
-        dj.phs = reinterpret_cast<const float2 *>(j.phs);
-        dj.k_r32 = j.k_r;
-        dj.k_r64 = j.k_r64;
-        dj.pos32 = j.pos;
-        dj.pos64 = j.pos64;
-        if (prec[i] == SARBP_PREC_PRECISE) {
-            if (!dj.k_r64 && !dj.k_r32) return fail(SARBP_ERR_INVALID, "k_r missing");
-            if (!dj.k_r32) dj.k_r32 = nullptr;
-        }
-        dj.r = j.r;
-        dj.u = j.u;
-        dj.v = j.v;
-        for (int k = 0; k < 3; ++k) {
-            dj.uh[k] = j.u_hat[k];
-            dj.vh[k] = j.v_hat[k];
-        }
+        describe_job(j, prec[i], L.tile_x, L.tile_y, dj);
         dj.Q = reinterpret_cast<float2 *>(sbase + lay[i].Q);
-        dj.Qp = rc_only ? nullptr : reinterpret_cast<float4 *>(sbase + lay[i].Qp);
+        dj.Qp = rc_only ? nullptr
+                : resident(i) ? const_cast<float4 *>(resident_qp[i])
+                              : reinterpret_cast<float4 *>(sbase + lay[i].Qp);
         dj.tiles = reinterpret_cast<TileInfo *>(sbase + lay[i].tiles);
         dj.recs = reinterpret_cast<PulseRec *>(sbase + lay[i].recs);
         dj.fin = reinterpret_cast<float2 *>(sbase + lay[i].fin);
@@ -392,17 +424,6 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         dj.wP = reinterpret_cast<float *>(sbase + lay[i].wP);
         dj.pulse = reinterpret_cast<double4 *>(sbase + lay[i].pulse);
         dj.sc = reinterpret_cast<JobScalars *>(sbase) + i;
-        dj.delta_r = j.delta_r;
-        // backprojection.cpp:120 and :53: lsa = floor(-S*dr/2), lsb = floor(S*dr/2),
-        // lsr = (lsb - lsa) / (N_fft - 1)
-        dj.lsa = std::floor((double)(-j.nsamples) * j.delta_r / 2);
-        const double lsb = std::floor((double)j.nsamples * j.delta_r / 2);
-        dj.lsr = (lsb - dj.lsa) / (double)(j.n_fft - 1);
-        dj.inv_lsr = 1.0 / dj.lsr;
-        dj.out = reinterpret_cast<double2 *>(j.output_img);
-        dj.out_u8 = j.out_u8;
-        dj.dB_min = j.dB_min;
-        dj.dB_max = j.dB_max;
     }
     RowItem *hr = reinterpret_cast<RowItem *>(h + o_rows);
     std::vector<std::pair<int, size_t>> row_groups;  // (logN, first row)

@@ -31,6 +31,9 @@ struct DeviceBuffer {
     size_t cap = 0;
     // Grows to at least `bytes`; synchronises `st` before freeing the old one.
     cudaError_t ensure(size_t bytes, cudaStream_t st);
+    // Frees any previous buffer (the caller makes sure it is idle) and
+    // allocates exactly `bytes`, rounded up to 256.
+    cudaError_t alloc_exact(size_t bytes);
     void release();
 };
 
@@ -103,14 +106,19 @@ public:
     // Runner must not enqueue anything else afterwards), and every buffer
     // must already be large enough (an uncaptured enqueue of the same jobs
     // comes first).
+    // With resident_qp, job i whose resident_qp[i] is non-NULL uses those
+    // range profiles (interpolation pairs [P][N+1], formed beforehand) and
+    // needs no phase history: its range compression is skipped.
     int enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cudaStream_t st,
-                void *q_out = nullptr, bool for_graph = false, const SlabSpec *slabs = nullptr);
+                void *q_out = nullptr, bool for_graph = false, const SlabSpec *slabs = nullptr,
+                const float4 *const *resident_qp = nullptr);
     // tile size the next enqueue with these options uses
     static void tile_shape(const sarbp_opts *opts, int *tile_x, int *tile_y);
     // Waits for the last batch and reads the kernels' status words.
     int check_status(cudaStream_t st);
     // Device footprint of the library scratch a job needs (bytes).
-    static size_t job_scratch_bytes(const sarbp_job &j, const sarbp_opts *opts = nullptr);
+    static size_t job_scratch_bytes(const sarbp_job &j, const sarbp_opts *opts = nullptr,
+                                    bool resident_profiles = false);
     // Frees the scratch (the Runner must be idle).
     void release_scratch() { scratch_.release(); }
     // Take each batch's scratch from `pool` (stream-ordered) instead of the
@@ -134,5 +142,13 @@ private:
 };
 
 BpLaunch default_launch(const sarbp_opts *opts, int num_sms);
+
+// Checks a job's sizes, pointers and Taylor level (SARBP_OK or an error code
+// with the message set); need_phs = false for pulse-chunked jobs, whose
+// phase history comes chunk by chunk.
+int validate_job(const sarbp_job &j, int prec, int idx, bool rc_only, bool need_phs);
+// Fills the sizes, Taylor coefficients, caller pointers, range-axis
+// constants and outputs of a job's descriptor (not its scratch pointers).
+void describe_job(const sarbp_job &j, int prec, int tile_x, int tile_y, DevJob &dj);
 
 }  // namespace sarbp

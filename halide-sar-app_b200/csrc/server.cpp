@@ -22,9 +22,18 @@
 // batch launches and returned stream-ordered behind it; the budget is
 // charged from admission to completion.  A request larger than the whole
 // budget fails with SARBP_ERR_ADMISSION.
+//
+// Registered apertures: sarbp_server_register uploads a phase history, k_r
+// and antenna positions once and range-compresses them once into resident
+// interpolation pairs; requests submitted on the aperture
+// (sarbp_server_submit_on) bring only their image plane and outputs, and
+// their batches skip the upload and the range compression of that aperture.
+// The resident bytes are charged to the budget from registration to
+// sarbp_server_unregister.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -48,8 +57,22 @@ using Clock = std::chrono::steady_clock;
 
 size_t a256(size_t x) { return (x + 255) / 256 * 256; }
 
+// A registered aperture: device copies of k_r and the antenna positions and
+// the range profiles as interpolation pairs [P][N_fft + 1] (one block).
+struct Aperture {
+    long long id = 0;
+    sarbp_job shape{};  // sizes, Taylor, delta_r and precision of the aperture
+    void *mem = nullptr;
+    size_t bytes = 0;
+    const float *k32 = nullptr, *p32 = nullptr;
+    const double *k64 = nullptr, *p64 = nullptr;
+    const float4 *qp = nullptr;
+    int refs = 0;  // queued or running requests on it
+};
+
 struct Request {
     long long id = 0;
+    Aperture *ap = nullptr;  // registered aperture, or NULL (the request brings its phase history)
     sarbp_job host{};  // the caller's job, host pointers
     size_t io_bytes = 0, scratch_bytes = 0;
     double work = 0.0;  // pixel*pulses
@@ -69,7 +92,7 @@ IoLayout io_layout(const sarbp_job &j) {
     const size_t P = (size_t)j.npulses, S = (size_t)j.nsamples, npix = (size_t)j.nu * j.nv;
     IoLayout L{};
     size_t o = 0;
-    L.phs = o; o += a256(P * S * 8);
+    L.phs = o; o += j.phs ? a256(P * S * 8) : 0;
     L.k32 = o; o += j.k_r ? a256(S * 4) : 0;
     L.k64 = o; o += j.k_r64 ? a256(S * 8) : 0;
     L.p32 = o; o += j.pos ? a256(P * 12) : 0;
@@ -114,6 +137,13 @@ struct sarbp_server {
     std::deque<Lane *> inflight;
     bool stop = false, sched_exited = false;
     std::thread sched, comp;
+    // registered apertures (guarded by mu) and their set-up stream
+    std::map<long long, std::unique_ptr<Aperture>> apertures;
+    long long next_ap = 1;
+    cudaStream_t reg_st = nullptr;
+    // counters: bytes copied host -> device, pulses range-compressed,
+    // requests served from a registered aperture
+    std::atomic<long long> h2d_bytes{0}, rc_pulses{0}, resident_requests{0};
 
     double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 
@@ -125,9 +155,11 @@ struct sarbp_server {
 void sarbp_server::launch_batch(Lane &L) {
     cudaSetDevice(ctx->dev.device);
     std::vector<sarbp_job> jobs;
+    std::vector<const float4 *> resident;
     jobs.reserve(L.batch.size());
     int rc = SARBP_OK;
     std::string err;
+    long long up = 0, rcp = 0, res = 0;
     for (Request *q : L.batch) {
         const sarbp_job &h = q->host;
         const IoLayout lay = io_layout(h);
@@ -147,18 +179,32 @@ void sarbp_server::launch_batch(Lane &L) {
                            {lay.u, h.r ? nullptr : h.u, (size_t)h.nu * 8},
                            {lay.v, h.r ? nullptr : h.v, (size_t)h.nv * 8}};
         for (const Copy &c : in)
-            if (c.src && e == cudaSuccess) e = cudaMemcpyAsync(b + c.off, c.src, c.n, cudaMemcpyHostToDevice, L.st);
+            if (c.src && e == cudaSuccess) {
+                e = cudaMemcpyAsync(b + c.off, c.src, c.n, cudaMemcpyHostToDevice, L.st);
+                up += (long long)c.n;
+            }
         if (e != cudaSuccess) {
             rc = cuda_fail(e, "serving: uploading a request");
             err = last_error_cstr();
             break;
         }
         sarbp_job d = h;
-        d.phs = reinterpret_cast<const float *>(b + lay.phs);
-        d.k_r = h.k_r ? reinterpret_cast<const float *>(b + lay.k32) : nullptr;
-        d.k_r64 = h.k_r64 ? reinterpret_cast<const double *>(b + lay.k64) : nullptr;
-        d.pos = h.pos ? reinterpret_cast<const float *>(b + lay.p32) : nullptr;
-        d.pos64 = h.pos64 ? reinterpret_cast<const double *>(b + lay.p64) : nullptr;
+        if (q->ap) {  // resident phase history: no upload, no range compression
+            d.phs = nullptr;
+            d.k_r = q->ap->k32;
+            d.k_r64 = q->ap->k64;
+            d.pos = q->ap->p32;
+            d.pos64 = q->ap->p64;
+            ++res;
+        } else {
+            d.phs = reinterpret_cast<const float *>(b + lay.phs);
+            d.k_r = h.k_r ? reinterpret_cast<const float *>(b + lay.k32) : nullptr;
+            d.k_r64 = h.k_r64 ? reinterpret_cast<const double *>(b + lay.k64) : nullptr;
+            d.pos = h.pos ? reinterpret_cast<const float *>(b + lay.p32) : nullptr;
+            d.pos64 = h.pos64 ? reinterpret_cast<const double *>(b + lay.p64) : nullptr;
+            rcp += h.npulses;
+        }
+        resident.push_back(q->ap ? q->ap->qp : nullptr);
         d.r = h.r ? reinterpret_cast<const double *>(b + lay.r) : nullptr;
         d.u = (!h.r && h.u) ? reinterpret_cast<const double *>(b + lay.u) : nullptr;
         d.v = (!h.r && h.v) ? reinterpret_cast<const double *>(b + lay.v) : nullptr;
@@ -167,9 +213,13 @@ void sarbp_server::launch_batch(Lane &L) {
         jobs.push_back(d);
     }
     if (rc == SARBP_OK) {
-        rc = L.runner->enqueue(jobs.data(), (int)jobs.size(), &launch, L.st);
+        rc = L.runner->enqueue(jobs.data(), (int)jobs.size(), &launch, L.st, nullptr, false, nullptr,
+                               resident.data());
         if (rc) err = last_error_cstr();
     }
+    h2d_bytes += up;
+    rc_pulses += rcp;
+    resident_requests += res;
     if (rc == SARBP_OK) {
         for (size_t i = 0; i < jobs.size() && rc == SARBP_OK; ++i) {
             const sarbp_job &h = L.batch[i]->host;
@@ -229,6 +279,7 @@ void sarbp_server::scheduler() {
                                std::to_string(cap >> 20) + " MiB";
                     q->done = true;
                     q->t_done = now();
+                    if (q->ap) --q->ap->refs;
                     ++completed;
                     cv.notify_all();
                     continue;
@@ -293,6 +344,7 @@ void sarbp_server::completer() {
                 q->status = rc;
                 q->error = err;
             }
+            if (q->ap) --q->ap->refs;
             q->t_done = t;
             q->done = true;
             ++completed;
@@ -338,6 +390,7 @@ int sarbp_server_create(sarbp_ctx *ctx, const sarbp_opts *launch, double hbm_cap
         L.runner->stage_events = false;
         L.runner->use_pool(s->pool);
     }
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->reg_st, cudaStreamNonBlocking);
     if (e == cudaSuccess) {
         // back the pool with memory up front so that first batches do not
         // pay for physical allocation (kept: the release threshold is the cap)
@@ -352,6 +405,7 @@ int sarbp_server_create(sarbp_ctx *ctx, const sarbp_opts *launch, double hbm_cap
             if (L.st) cudaStreamDestroy(L.st);
             if (L.done) cudaEventDestroy(L.done);
         }
+        if (s->reg_st) cudaStreamDestroy(s->reg_st);
         cudaMemPoolDestroy(s->pool);
         return cuda_fail(e, "creating serving lanes");
     }
@@ -448,8 +502,214 @@ int sarbp_server_destroy(sarbp_server *s) {
         if (L.st) cudaStreamDestroy(L.st);
         if (L.done) cudaEventDestroy(L.done);
     }
+    for (auto &kv : s->apertures) cudaFreeAsync(kv.second->mem, s->reg_st);
+    s->apertures.clear();
+    if (s->reg_st) {
+        cudaStreamSynchronize(s->reg_st);
+        cudaStreamDestroy(s->reg_st);
+    }
     if (s->pool) cudaMemPoolDestroy(s->pool);
     delete s;
+    return SARBP_OK;
+}
+
+int sarbp_server_register(sarbp_server *s, const sarbp_job *host_aperture, long long *aperture) {
+    if (!s || !host_aperture || !aperture) return fail(SARBP_ERR_INVALID, "bad register arguments");
+    int rc = ctx_set_device(s->ctx);
+    if (rc) return rc;
+    sarbp_job h = *host_aperture;
+    if (h.precision < 0) h.precision = s->launch.precision;
+    if (h.precision != SARBP_PREC_COMPAT && h.precision != SARBP_PREC_PRECISE)
+        return fail(SARBP_ERR_UNSUPPORTED, "registered apertures run SARBP_PREC_COMPAT or SARBP_PREC_PRECISE");
+    // the image plane is the requests' business: check the rest with a stand-in one
+    sarbp_job chk = h;
+    chk.nu = chk.nv = 1;
+    chk.r = nullptr;
+    chk.u = chk.v = reinterpret_cast<const double *>(&h);
+    chk.output_img = reinterpret_cast<double *>(&chk);
+    chk.out_u8 = nullptr;
+    rc = validate_job(chk, h.precision, 0, false, true);
+    if (rc) return rc;
+    const size_t P = (size_t)h.npulses, S = (size_t)h.nsamples, N = (size_t)h.n_fft;
+    // resident block [k32][k64][p32][p64][pairs]; set-up block
+    // [phs][scalars][descriptor][filt][wS][wP][pulse][rows]
+    const size_t b_k32 = h.k_r ? a256(S * 4) : 0, b_k64 = h.k_r64 ? a256(S * 8) : 0;
+    const size_t b_p32 = h.pos ? a256(P * 12) : 0, b_p64 = h.pos64 ? a256(P * 24) : 0;
+    const size_t b_qp = a256(P * (N + 1) * sizeof(float4));
+    const size_t res_bytes = b_k32 + b_k64 + b_p32 + b_p64 + b_qp;
+    const size_t o_sc = a256(P * S * 8), o_job = o_sc + a256(sizeof(JobScalars));
+    const size_t o_filt = o_job + a256(sizeof(DevJob)), o_ws = o_filt + a256(S * 4), o_wp = o_ws + a256(S * 4);
+    const size_t o_pulse = o_wp + a256(P * 4), o_rows = o_pulse + a256(P * sizeof(double4));
+    const size_t tmp_bytes = o_rows + a256(P * sizeof(RowItem));
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->in_use + res_bytes + tmp_bytes > s->cap)
+            return fail(SARBP_ERR_ADMISSION, "registering needs " + std::to_string((res_bytes + tmp_bytes) >> 20) +
+                                                 " MiB of device memory; the budget has " +
+                                                 std::to_string((s->cap - std::min(s->cap, s->in_use)) >> 20) +
+                                                 " MiB free");
+        s->in_use += res_bytes + tmp_bytes;
+        s->peak = std::max(s->peak, s->in_use);
+    }
+    auto uncharge = [&](size_t bytes) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->in_use -= bytes;
+        s->cv.notify_all();
+    };
+    cudaStream_t st = s->reg_st;
+    auto ap = std::make_unique<Aperture>();
+    void *tmp = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&ap->mem, res_bytes, s->pool, st);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&tmp, tmp_bytes, s->pool, st);
+    if (e != cudaSuccess) {
+        if (ap->mem) cudaFreeAsync(ap->mem, st);
+        cudaStreamSynchronize(st);
+        uncharge(res_bytes + tmp_bytes);
+        return cuda_fail(e, "registering an aperture: device memory");
+    }
+    char *rb = static_cast<char *>(ap->mem), *tb = static_cast<char *>(tmp);
+    size_t o = 0;
+    struct Copy { const void *src; size_t n, b; char *dst; };
+    const Copy in[] = {{h.k_r, S * 4, b_k32, nullptr}, {h.k_r64, S * 8, b_k64, nullptr},
+                       {h.pos, P * 12, b_p32, nullptr}, {h.pos64, P * 24, b_p64, nullptr}};
+    char *dst[4] = {};
+    for (int i = 0; i < 4 && e == cudaSuccess; ++i) {
+        if (!in[i].src) continue;
+        dst[i] = rb + o;
+        e = cudaMemcpyAsync(dst[i], in[i].src, in[i].n, cudaMemcpyHostToDevice, st);
+        o += in[i].b;
+    }
+    ap->k32 = reinterpret_cast<const float *>(dst[0]);
+    ap->k64 = reinterpret_cast<const double *>(dst[1]);
+    ap->p32 = reinterpret_cast<const float *>(dst[2]);
+    ap->p64 = reinterpret_cast<const double *>(dst[3]);
+    ap->qp = reinterpret_cast<const float4 *>(rb + o);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(tb, h.phs, P * S * 8, cudaMemcpyHostToDevice, st);
+    // range compression into the resident pairs (prep kernel: windows, filter)
+    sarbp_job d = h;
+    d.phs = reinterpret_cast<const float *>(tb);
+    d.k_r = ap->k32;
+    d.k_r64 = ap->k64;
+    d.pos = ap->p32;
+    d.pos64 = ap->p64;
+    DevJob dj{};
+    describe_job(d, h.precision, 32, 32, dj);
+    dj.Qp = const_cast<float4 *>(ap->qp);
+    dj.sc = reinterpret_cast<JobScalars *>(tb + o_sc);
+    dj.filt = reinterpret_cast<float *>(tb + o_filt);
+    dj.wS = reinterpret_cast<float *>(tb + o_ws);
+    dj.wP = reinterpret_cast<float *>(tb + o_wp);
+    dj.pulse = reinterpret_cast<double4 *>(tb + o_pulse);
+    DevJob *d_job = reinterpret_cast<DevJob *>(tb + o_job);
+    auto *rows = reinterpret_cast<RowItem *>(tb + o_rows);
+    float2 *tw = nullptr;
+    if (e == cudaSuccess) e = s->ctx->dev.twiddle(dj.logN, &tw);
+    if (e == cudaSuccess) e = launch_store_job(dj, d_job, st);
+    if (e == cudaSuccess) {
+        launch_prep(d_job, 1, st);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = launch_fill_items(nullptr, 0, rows, (int)P, st);
+    if (e == cudaSuccess) e = launch_range_compress(dj.logN, d_job, rows, (int)P, 1, tw, st);
+    if (e == cudaSuccess) e = cudaFreeAsync(tmp, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cudaStreamSynchronize(st);
+        cudaFreeAsync(ap->mem, st);
+        cudaStreamSynchronize(st);
+        uncharge(res_bytes + tmp_bytes);
+        return cuda_fail(e, "registering an aperture: upload and range compression");
+    }
+    s->ctx->dev.launches += 4;
+    s->h2d_bytes += (long long)(P * S * 8 + (h.k_r ? S * 4 : 0) + (h.k_r64 ? S * 8 : 0) + (h.pos ? P * 12 : 0) +
+                                (h.pos64 ? P * 24 : 0));
+    s->rc_pulses += (long long)P;
+    ap->shape = h;
+    ap->shape.phs = nullptr;
+    ap->bytes = res_bytes;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->in_use -= tmp_bytes;
+    ap->id = s->next_ap++;
+    *aperture = ap->id;
+    s->apertures[ap->id] = std::move(ap);
+    s->cv.notify_all();
+    return SARBP_OK;
+}
+
+int sarbp_server_submit_on(sarbp_server *s, long long aperture, const sarbp_job *host_job, long long *id) {
+    if (!s || !host_job || !id) return fail(SARBP_ERR_INVALID, "bad submit arguments");
+    const sarbp_job &j = *host_job;
+    if (j.nu < 1 || j.nv < 1 || !(j.r || (j.u && j.v)))
+        return fail(SARBP_ERR_INVALID, "request: nu, nv and pixel positions are required");
+    auto q = std::make_unique<Request>();
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) return fail(SARBP_ERR_STATE, "server is shutting down");
+    auto it = s->apertures.find(aperture);
+    if (it == s->apertures.end()) return fail(SARBP_ERR_INVALID, "unknown aperture id");
+    Aperture *ap = it->second.get();
+    sarbp_job h = ap->shape;  // sizes, Taylor, delta_r, precision
+    h.phs = nullptr;
+    h.k_r = nullptr;
+    h.k_r64 = nullptr;
+    h.pos = nullptr;
+    h.pos64 = nullptr;
+    h.nu = j.nu;
+    h.nv = j.nv;
+    h.r = j.r;
+    h.u = j.u;
+    h.v = j.v;
+    for (int k = 0; k < 3; ++k) {
+        h.u_hat[k] = j.u_hat[k];
+        h.v_hat[k] = j.v_hat[k];
+    }
+    h.output_img = j.output_img;
+    h.out_u8 = j.out_u8;
+    h.dB_min = j.dB_min;
+    h.dB_max = j.dB_max;
+    q->host = h;
+    q->ap = ap;
+    q->io_bytes = io_layout(h).end;
+    q->scratch_bytes = Runner::job_scratch_bytes(h, &s->launch, true) + (64u << 10);
+    q->work = (double)h.nu * h.nv * h.npulses;
+    ++ap->refs;
+    q->id = s->next_id++;
+    q->t_submit = s->now();
+    *id = q->id;
+    s->queue.push_back(q.get());
+    s->reqs[q->id] = std::move(q);
+    ++s->submitted;
+    s->cv.notify_all();
+    return SARBP_OK;
+}
+
+int sarbp_server_unregister(sarbp_server *s, long long aperture) {
+    if (!s) return fail(SARBP_ERR_INVALID, "server is NULL");
+    std::unique_ptr<Aperture> ap;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->apertures.find(aperture);
+        if (it == s->apertures.end()) return fail(SARBP_ERR_INVALID, "unknown aperture id");
+        if (it->second->refs > 0)
+            return fail(SARBP_ERR_STATE, "aperture still has queued or running requests");
+        ap = std::move(it->second);
+        s->apertures.erase(it);
+    }
+    cudaSetDevice(s->ctx->dev.device);
+    cudaError_t e = cudaFreeAsync(ap->mem, s->reg_st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->reg_st);
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->in_use -= ap->bytes;
+    s->cv.notify_all();
+    if (e != cudaSuccess) return cuda_fail(e, "unregistering an aperture");
+    return SARBP_OK;
+}
+
+int sarbp_server_counters(sarbp_server *s, double *h2d_bytes, long long *rc_pulses,
+                          long long *resident_requests) {
+    if (!s) return fail(SARBP_ERR_INVALID, "server is NULL");
+    if (h2d_bytes) *h2d_bytes = (double)s->h2d_bytes.load();
+    if (rc_pulses) *rc_pulses = s->rc_pulses.load();
+    if (resident_requests) *resident_requests = s->resident_requests.load();
     return SARBP_OK;
 }
 

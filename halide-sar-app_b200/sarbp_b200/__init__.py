@@ -20,11 +20,12 @@ import math
 import numpy as np
 
 from ._lib import (ERR_ADMISSION, ERR_CUDA, ERR_GEOMETRY, ERR_INVALID, ERR_NOMEM, ERR_STATE,
-                   ERR_TIMEOUT, ERR_UNSUPPORTED, OK, PREC_COMPAT, PREC_NAIVE, PREC_PRECISE, Job,
-                   Opts, SarbpError, check, lib)
+                   ERR_TIMEOUT, ERR_UNSUPPORTED, OK, PREC_COMPAT, PREC_NAIVE, PREC_PRECISE,
+                   TAYLOR_FLOAT, TAYLOR_REF, Job, Opts, SarbpError, check, lib)
 
 __all__ = [
     "Context", "Job", "Opts", "SarbpError", "PREC_COMPAT", "PREC_PRECISE", "PREC_NAIVE",
+    "TAYLOR_REF", "TAYLOR_FLOAT",
     "n_fft_for", "taylor", "img_plane_create", "img_plane_dims", "pixel_locs", "version",
 ]
 
@@ -47,9 +48,14 @@ def n_fft_for(nsamples, upsample):
     return int(math.pow(2, int(math.log2(nsamples * upsample)) + 1))
 
 
-def taylor(num, S_L):
+def taylor(num, S_L, mode=TAYLOR_REF):
+    """Taylor window (signal.h:14-51); mode TAYLOR_FLOAT takes the F_m
+    denominator quotient in floating point instead of Int32."""
     out = np.empty(num, np.float64)
-    check(lib().sarbp_taylor(int(num), float(S_L), _ptr(out)))
+    if mode == TAYLOR_REF:
+        check(lib().sarbp_taylor(int(num), float(S_L), _ptr(out)))
+    else:
+        check(lib().sarbp_taylor_mode(int(num), float(S_L), int(mode), _ptr(out)))
     return out
 
 
@@ -228,6 +234,12 @@ class Context:
                                         _ptr(out)))
         return out
 
+    def img_output_u8_from_img_device(self, img_ptr, nu, nv, dB_min, dB_max, out_ptr):
+        """u8 image [nv, nu] from a device complex128 image in one pass (max|z|
+        reduction + grey levels), enqueued on the context's stream."""
+        check(lib().sarbp_img_output_u8_from_img_device(self._h, ctypes.c_void_p(img_ptr), int(nu), int(nv),
+                                                        float(dB_min), float(dB_max), ctypes.c_void_p(out_ptr)))
+
     def range_compress_device(self, job, q_out_ptr, precision=None):
         """Writes the complex64 range profiles [P, N_fft] of `job` to q_out_ptr."""
         o = _opts(precision)
@@ -260,6 +272,74 @@ class Context:
         return Plan(self, jobs, precision, **tune)
 
 
+class Accumulator:
+    """Pulse-chunked image formation (sarbp_accum_*): a device-resident
+    partial image that takes the aperture's phase-history rows chunk by
+    chunk.  `job` is a Job of device pointers for the whole aperture (its
+    phs field is not read); add_device(pulse0, count, ptr) takes device rows,
+    add(pulse0, rows) host rows (complex64 [count, S]); finalize() writes the
+    job's output image; wait() returns once done (raises on a kernel error)."""
+
+    def __init__(self, ctx, job, max_chunk, precision=None, **tune):
+        self._job = job
+        o = _opts(precision, **tune)
+        self._h = ctypes.c_void_p()
+        check(lib().sarbp_accum_create(ctx._h, ctypes.byref(job), ctypes.byref(o), int(max_chunk),
+                                       ctypes.byref(self._h)))
+        self._rows = []
+
+    def add_device(self, pulse0, count, phs_rows_ptr):
+        check(lib().sarbp_accum_add_device(self._h, int(pulse0), int(count), ctypes.c_void_p(phs_rows_ptr)))
+
+    def add(self, pulse0, rows):
+        rows = np.ascontiguousarray(rows, np.complex64)
+        check(lib().sarbp_accum_add(self._h, int(pulse0), int(rows.shape[0]), _ptr(rows)))
+        self._rows = self._rows[-1:] + [rows]  # the copy may still read them
+
+    def finalize(self):
+        check(lib().sarbp_accum_finalize(self._h))
+
+    def wait(self):
+        check(lib().sarbp_accum_wait(self._h))
+        self._rows = []
+
+    def reset(self):
+        check(lib().sarbp_accum_reset(self._h))
+
+    @property
+    def device_bytes(self):
+        return float(lib().sarbp_accum_device_bytes(self._h))
+
+    def close(self):
+        if self._h:
+            lib().sarbp_accum_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def job_device_bytes(job, chunk_pulses=0, precision=None, **tune):
+    """Device bytes of a job formed in one call, or in chunks of chunk_pulses."""
+    b = ctypes.c_double()
+    o = _opts(precision, **tune)
+    check(lib().sarbp_job_device_bytes(ctypes.byref(job), ctypes.byref(o), int(chunk_pulses), ctypes.byref(b)))
+    return b.value
+
+
+def backprojection_streamed(ctx, host_job, max_device_bytes, precision=None, **tune):
+    """A Job of HOST pointers formed in pulse chunks under a device-memory
+    cap (sarbp_backprojection_streamed); returns (chunk pulses, device bytes)."""
+    o = _opts(precision, **tune)
+    c, b = ctypes.c_int(), ctypes.c_double()
+    check(lib().sarbp_backprojection_streamed(ctx._h, ctypes.byref(host_job), ctypes.byref(o),
+                                              float(max_device_bytes), ctypes.byref(c), ctypes.byref(b)))
+    return c.value, b.value
+
+
 class Server:
     """The serving loop (sarbp_server_*): submit(job) queues a Job whose
     pointers are host memory and returns its id; wait(id) returns its status
@@ -279,6 +359,31 @@ class Server:
         check(lib().sarbp_server_submit(self._h, ctypes.byref(job), ctypes.byref(rid)))
         self._keep[rid.value] = (job, keep)
         return rid.value
+
+    def register(self, job, keep=None):
+        """Uploads and range-compresses an aperture (a Job of host pointers)
+        once; returns its id for submit_on."""
+        aid = ctypes.c_longlong()
+        check(lib().sarbp_server_register(self._h, ctypes.byref(job), ctypes.byref(aid)))
+        return aid.value
+
+    def submit_on(self, aperture, job, keep=None):
+        """Queues a request on a registered aperture: `job` supplies the image
+        plane (nu, nv, r or u/v/u_hat/v_hat) and outputs, host memory."""
+        rid = ctypes.c_longlong()
+        check(lib().sarbp_server_submit_on(self._h, int(aperture), ctypes.byref(job), ctypes.byref(rid)))
+        self._keep[rid.value] = (job, keep)
+        return rid.value
+
+    def unregister(self, aperture):
+        check(lib().sarbp_server_unregister(self._h, int(aperture)))
+
+    def counters(self):
+        """(bytes copied host -> device, pulses range-compressed, requests
+        served from registered apertures) since the server started."""
+        b, p, r = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_longlong()
+        check(lib().sarbp_server_counters(self._h, ctypes.byref(b), ctypes.byref(p), ctypes.byref(r)))
+        return dict(h2d_bytes=b.value, rc_pulses=p.value, resident_requests=r.value)
 
     def wait(self, rid, timeout=-1.0):
         return int(lib().sarbp_server_wait(self._h, int(rid), float(timeout)))
@@ -345,7 +450,7 @@ class Plan:
 
 def make_job(nsamples, npulses, n_fft, taylor_s_l, nu, nv, delta_r, phs, k_r, pos, output_img,
              r=0, u=0, v=0, u_hat=(0, 0, 0), v_hat=(0, 0, 0), k_r64=0, pos64=0, out_u8=0,
-             dB_min=0.0, dB_max=0.0, precision=-1):
+             dB_min=0.0, dB_max=0.0, precision=-1, taylor_mode=TAYLOR_REF):
     """Builds a Job from device addresses (ints, e.g. tensor.data_ptr())."""
     j = Job()
     j.nsamples, j.npulses, j.n_fft, j.taylor_s_l = int(nsamples), int(npulses), int(n_fft), int(taylor_s_l)
@@ -358,4 +463,5 @@ def make_job(nsamples, npulses, n_fft, taylor_s_l, nu, nv, delta_r, phs, k_r, po
     j.output_img, j.out_u8 = output_img or None, out_u8 or None
     j.dB_min, j.dB_max = float(dB_min), float(dB_max)
     j.precision = int(precision)
+    j.taylor_mode = int(taylor_mode)
     return j

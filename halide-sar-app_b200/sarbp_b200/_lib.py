@@ -24,6 +24,9 @@ PREC_COMPAT = 0
 PREC_PRECISE = 1
 PREC_NAIVE = 2
 
+TAYLOR_REF = 0
+TAYLOR_FLOAT = 1
+
 _c_int_p = ctypes.POINTER(ctypes.c_int)
 _dp = ctypes.c_void_p
 
@@ -49,7 +52,7 @@ class Job(ctypes.Structure):
                 ("u_hat", ctypes.c_double * 3), ("v_hat", ctypes.c_double * 3),
                 ("output_img", _dp), ("out_u8", _dp),
                 ("dB_min", ctypes.c_double), ("dB_max", ctypes.c_double),
-                ("precision", ctypes.c_int), ("reserved", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("taylor_mode", ctypes.c_int)]
 
 
 # name -> (restype, argtypes); every symbol declared in include/sarbp_b200.h
@@ -97,6 +100,13 @@ SIGNATURES = {
                                           ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
                                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "sarbp_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "sarbp_server_register": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job),
+                                             ctypes.POINTER(ctypes.c_longlong)]),
+    "sarbp_server_submit_on": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(Job),
+                                              ctypes.POINTER(ctypes.c_longlong)]),
+    "sarbp_server_unregister": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
+    "sarbp_server_counters": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                             ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     "sarbp_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job), ctypes.c_int,
                                       ctypes.POINTER(Opts), ctypes.POINTER(ctypes.c_float)]),
     "sarbp_backprojection_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job),
@@ -106,6 +116,20 @@ SIGNATURES = {
     "sarbp_range_compress_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job),
                                                    ctypes.POINTER(Opts), _dp]),
     "sarbp_backprojection_noalloc": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.c_void_p, _dp]),
+    "sarbp_accum_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job), ctypes.POINTER(Opts),
+                                          ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "sarbp_accum_add_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp]),
+    "sarbp_accum_add": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp]),
+    "sarbp_accum_finalize": (ctypes.c_int, [ctypes.c_void_p]),
+    "sarbp_accum_wait": (ctypes.c_int, [ctypes.c_void_p]),
+    "sarbp_accum_reset": (ctypes.c_int, [ctypes.c_void_p]),
+    "sarbp_accum_device_bytes": (ctypes.c_double, [ctypes.c_void_p]),
+    "sarbp_accum_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "sarbp_job_device_bytes": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Opts), ctypes.c_int,
+                                              ctypes.POINTER(ctypes.c_double)]),
+    "sarbp_backprojection_streamed": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job), ctypes.POINTER(Opts),
+                                                     ctypes.c_double, ctypes.POINTER(ctypes.c_int),
+                                                     ctypes.POINTER(ctypes.c_double)]),
     "sarbp_img_output_to_dB": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, _dp]),
     "sarbp_img_output_u8": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_double, ctypes.c_double, _dp]),
@@ -113,7 +137,10 @@ SIGNATURES = {
                                                      ctypes.c_int, _dp]),
     "sarbp_img_output_u8_device": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int,
                                                   ctypes.c_double, ctypes.c_double, _dp]),
+    "sarbp_img_output_u8_from_img_device": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int,
+                                                           ctypes.c_double, ctypes.c_double, _dp]),
     "sarbp_taylor": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, _dp]),
+    "sarbp_taylor_mode": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp]),
     "sarbp_img_plane_dims": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _c_int_p,
                                             _c_int_p]),
     "sarbp_img_plane": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp,

@@ -29,7 +29,7 @@ class DeviceJob:
                             self.out.data_ptr(), u=self.u.data_ptr(), v=self.v.data_ptr(),
                             u_hat=d["u_hat"], v_hat=d["v_hat"],
                             out_u8=self.out_u8.data_ptr() if u8 else 0, dB_min=db[0], dB_max=db[1],
-                            precision=-1)
+                            precision=-1, taylor_mode=d.get("taylor_mode", 0))
         self.units = self.nu * self.nv * self.P
 
     def image(self):
@@ -81,4 +81,4 @@ class HostJob:
                         p(self.phs), p(self.k32), p(self.p32), p(out), u=p(self.u), v=p(self.v),
                         u_hat=d["u_hat"], v_hat=d["v_hat"], k_r64=p(self.k64), pos64=p(self.p64),
                         out_u8=p(out_u8) if out_u8 is not None else 0, dB_min=db[0], dB_max=db[1],
-                        precision=precision)
+                        precision=precision, taylor_mode=d.get("taylor_mode", 0))

@@ -24,7 +24,7 @@ import ctypes
 import numpy as np
 
 from . import img_plane_create, n_fft_for, pixel_locs
-from ._lib import check, lib
+from ._lib import TAYLOR_FLOAT, TAYLOR_REF, check, lib
 
 C = 299792458.0
 
@@ -107,12 +107,18 @@ def make(name="plain_small", seed=1, with_r=True, overrides=None, nthreads=0):
     return out
 
 
+def taylor_mode_for(level):
+    """The reference's Taylor window (TAYLOR_REF) where it is defined, up to
+    30 dB; above that its F_m denominator divides by zero (the Int32
+    division of signal.h:40) and the float-quotient window (TAYLOR_FLOAT)
+    is used."""
+    return TAYLOR_REF if level <= 30 else TAYLOR_FLOAT
+
+
 def batch_jobs(njobs=96, seed=7, sizes=(256, 512, 1024, 2048), pulses=(128, 2000),
-               samples=(256, 512, 1024), taylors=(17, 30), ranges=(5e3, 15e3), deps=(20.0, 50.0)):
-    """Parameters of uneven jobs (no data): list of dicts.  Taylor levels stop
-    at 30 dB: above it the reference's window has non-finite coefficients
-    (the Int32 division in F_m's denominator, signal.h:14-51), which the
-    library rejects."""
+               samples=(256, 512, 1024), taylors=(17, 35), ranges=(5e3, 15e3), deps=(20.0, 50.0)):
+    """Parameters of uneven jobs (no data): list of dicts.  Taylor levels
+    17-35 dB; each job's taylor_mode is taylor_mode_for(level)."""
     rng = np.random.default_rng(seed)
     jobs = []
     for i in range(njobs):
@@ -129,6 +135,7 @@ def batch_jobs(njobs=96, seed=7, sizes=(256, 512, 1024, 2048), pulses=(128, 2000
                          clutter=0, snr=20.0, n=n, extent=extent,
                          taylor=int(rng.integers(taylors[0], taylors[1] + 1)), upsample=2,
                          db=(-40.0, 0.0), seed=int(seed * 1000 + i)))
+        jobs[-1]["taylor_mode"] = taylor_mode_for(jobs[-1]["taylor"])
     return jobs
 
 
@@ -141,7 +148,7 @@ def make_from(cfg, with_r=False, nthreads=0):
     g = grid_plane(cfg["n"], cfg["extent"], pos, delta_r, cfg["S"], cfg["P"])
     out = dict(cfg=cfg, phs=phs, pos=pos, k_r=k_r, delta_r=delta_r,
                N_fft=n_fft_for(cfg["S"], cfg["upsample"]), taylor=cfg["taylor"], db=cfg["db"],
-               scat=scat, S=cfg["S"], P=cfg["P"], **g)
+               taylor_mode=cfg.get("taylor_mode", TAYLOR_REF), scat=scat, S=cfg["S"], P=cfg["P"], **g)
     if with_r:
         out["r"] = pixel_locs(g["u"], g["v"], g["u_hat"], g["v_hat"])
     return out

@@ -53,6 +53,17 @@ extern "C" {
 #define SARBP_PREC_NAIVE 2   /* plain FP32 range and phase per pixel*pulse
                                 (precision-study baseline) */
 
+/* Taylor window of range compression (signal.h:14-51). */
+#define SARBP_TAYLOR_REF 0   /* the reference's expression as Halide types it:
+                                the F_m denominator term (m+1)^2/(r+1)^2 is an
+                                Int32 division (signal.h:40), which is zero-
+                                divided, so undefined, above 30 dB; such levels
+                                are rejected with SARBP_ERR_INVALID */
+#define SARBP_TAYLOR_FLOAT 1 /* the same window with that quotient taken in
+                                floating point (the published RITSAR taylor()
+                                the reference restates); defined at every level.
+                                A deviation from the reference, chosen per job. */
+
 typedef struct sarbp_ctx sarbp_ctx;
 
 /* Kernel tuning; a zero field means "library default / autotuned". */
@@ -89,7 +100,7 @@ typedef struct sarbp_job {
     uint8_t *out_u8;     /* optional: u8 image [nv][nu] (device), or NULL */
     double dB_min, dB_max; /* used when out_u8 != NULL */
     int precision;       /* SARBP_PREC_*; overrides opts->precision when >= 0 */
-    int reserved;
+    int taylor_mode;     /* SARBP_TAYLOR_REF (0) or SARBP_TAYLOR_FLOAT */
 } sarbp_job;
 
 /* ---- context ---- */
@@ -231,6 +242,108 @@ int sarbp_server_stats(sarbp_server *server, long long *submitted,
 int sarbp_server_destroy(sarbp_server *server);
 
 /*
+ * Registered apertures: the phase history of `host_aperture` (HOST
+ * pointers: phs, k_r and/or k_r64, pos and/or pos64; sizes, n_fft, Taylor
+ * level and mode, delta_r, precision -- <0: the server's) is uploaded and
+ * range-compressed ONCE, on the calling thread, and stays resident on the
+ * device as interpolation pairs (16 B x npulses x (n_fft + 1)) with its k_r
+ * and positions, charged to the server's budget until unregistered
+ * (SARBP_ERR_ADMISSION when it does not fit).  Requests submitted on it
+ * with sarbp_server_submit_on bring only their image plane (nu, nv, and r or
+ * u/v/u_hat/v_hat) and outputs (output_img, out_u8 with dB_min/dB_max), all
+ * host memory; the rest of host_job is ignored.  Their batches neither
+ * upload nor range-compress the phase history.  An aperture can be
+ * unregistered once none of its requests is queued or running.
+ */
+int sarbp_server_register(sarbp_server *server, const sarbp_job *host_aperture,
+                          long long *aperture);
+int sarbp_server_submit_on(sarbp_server *server, long long aperture,
+                           const sarbp_job *host_job, long long *id);
+int sarbp_server_unregister(sarbp_server *server, long long aperture);
+/* Bytes the server copied host -> device, pulses it range-compressed, and
+ * requests it served from registered apertures, since it started. */
+int sarbp_server_counters(sarbp_server *server, double *h2d_bytes,
+                          long long *rc_pulses, long long *resident_requests);
+
+/*
+ * Pulse-chunked image formation (no counterpart in the reference, which
+ * range-compresses and backprojects all pulses of a job in one call,
+ * backprojection.cpp:67-138): a device-resident partial image that
+ * accumulates the aperture's pulses chunk by chunk, for apertures whose
+ * phase history arrives over time or whose one-shot scratch (16 B x P x
+ * n_fft of range profiles and 32 B x P per 32x32-pixel tile of pulse
+ * geometry) does not fit.  The image is the reference's: a sum over pulses
+ * followed by the final phase of pulse P/2 and the row flip
+ * (backprojection.cpp:126-135), with the reference's pulse pairing
+ * (phase-history row q weighs w_P[q] and meets antenna position
+ * (q - P mod 2) mod P, from the double fftshift of backprojection.cpp:98,104).
+ *
+ * sarbp_accum_create: `job` holds device pointers and the WHOLE aperture's
+ *   sizes (npulses = P), k_r, antenna positions of all P pulses, Taylor
+ *   level, pixel positions (r, or u/v/u_hat/v_hat) and outputs (output_img,
+ *   optional out_u8); job->phs is not read.  The pointers must stay valid
+ *   until destroy.  Device memory: the windows, pulse and tile tables, the
+ *   final phase and a complex f32 partial image (8 B per pixel each), plus
+ *   scratch for one chunk of up to max_chunk pulses.  Enqueues its set-up
+ *   on the context's stream.  SARBP_PREC_COMPAT or SARBP_PREC_PRECISE.
+ * sarbp_accum_add_device: range-compresses phase-history rows
+ *   [pulse0, pulse0 + count) (phs_rows: complex64 [count][nsamples] on the
+ *   device, count <= max_chunk) and adds them to the partial image.
+ *   Chunks may come in any order; each pulse exactly once (again:
+ *   SARBP_ERR_STATE).  Enqueued on the context's stream.
+ * sarbp_accum_add: the same from host memory: the rows go up on the
+ *   context's copy stream into one of two staging buffers while the
+ *   previous chunk computes.  With pinned memory the copy is asynchronous:
+ *   keep the rows unchanged until the next sarbp_accum_add or
+ *   sarbp_accum_wait returns.
+ * sarbp_accum_finalize: once all P pulses are in, enqueues the final phase
+ *   and row flip into output_img (and the u8 image).
+ * sarbp_accum_wait: waits for the accumulator's work; after finalize,
+ *   returns the kernels' status as sarbp_ctx_synchronize does.
+ * sarbp_accum_reset: zeroes the partial image for a new aperture on the
+ *   same geometry (same positions, pixels and sizes).
+ */
+typedef struct sarbp_accum sarbp_accum;
+int sarbp_accum_create(sarbp_ctx *ctx, const sarbp_job *job,
+                       const sarbp_opts *opts, int max_chunk,
+                       sarbp_accum **out);
+int sarbp_accum_add_device(sarbp_accum *acc, int pulse0, int count,
+                           const float *phs_rows);
+int sarbp_accum_add(sarbp_accum *acc, int pulse0, int count,
+                    const float *phs_rows_host);
+int sarbp_accum_finalize(sarbp_accum *acc);
+int sarbp_accum_wait(sarbp_accum *acc);
+int sarbp_accum_reset(sarbp_accum *acc);
+/* device bytes the accumulator holds (with its staging buffers) */
+double sarbp_accum_device_bytes(const sarbp_accum *acc);
+int sarbp_accum_destroy(sarbp_accum *acc);
+
+/*
+ * Device bytes a job needs: its inputs and outputs plus the library's
+ * scratch, formed in one call (chunk_pulses <= 0 or >= npulses) or in
+ * pulse chunks of chunk_pulses with two staging buffers (the phase history
+ * itself then never resides whole).
+ */
+int sarbp_job_device_bytes(const sarbp_job *job, const sarbp_opts *opts,
+                           int chunk_pulses, double *bytes);
+
+/*
+ * A job with HOST pointers (as for the serving loop) formed under a device
+ * memory cap: picks the largest pulse chunk whose footprint
+ * (sarbp_job_device_bytes) fits max_device_bytes, evens the chunks out,
+ * uploads the inputs other than the phase history, streams the phase
+ * history chunk by chunk (each upload overlapped with the previous chunk's
+ * kernels) through a pulse-chunked accumulator, and copies the image (and
+ * u8 image) back.  *chunk_pulses and *device_bytes (either may be NULL)
+ * receive the chunk size used and the device memory held.  Returns when the
+ * image is on the host.
+ */
+int sarbp_backprojection_streamed(sarbp_ctx *ctx, const sarbp_job *host_job,
+                                  const sarbp_opts *opts,
+                                  double max_device_bytes, int *chunk_pulses,
+                                  double *device_bytes);
+
+/*
  * Launch-shape autotuner: runs the batch with each candidate pixel tile
  * (32x32, 32x16, 64x16, 16x32 at 3 CTAs/SM; 32x32, 32x64, 64x32, 16x64 at
  * 2, with the staging buffer grown into the third CTA's shared memory) and
@@ -246,21 +359,29 @@ int sarbp_autotune(sarbp_ctx *ctx, const sarbp_job *jobs, int njobs,
 
 /*
  * Backprojection of one device-resident job that allocates nothing (no
- * counterpart in the reference).  For callers that cannot allocate device
- * memory when they need an image -- inside a stream capture, under a memory
- * pool they do not own, or in a loop that must not touch the allocator.
- * Runs the same kernels as sarbp_backprojection_device on `cuda_stream`,
- * with all scratch in one static 64 MiB device array of the library:
+ * counterpart in the reference).  For callers that must not allocate device
+ * memory when they need an image: processes whose device memory is handed
+ * out up front by a pool they do not own (a cudaMalloc there fails, or
+ * fragments and bypasses the pool), and real-time loops that cannot take
+ * cudaMalloc's latency and implicit device synchronisation on the path that
+ * forms each image.  Runs the same kernels as sarbp_backprojection_device on
+ * `cuda_stream`, with all scratch in one static 64 MiB device array of the
+ * library:
  *  - jobs needing more scratch than that return SARBP_ERR_UNSUPPORTED
- *    (roughly: 16 B x npulses x n_fft + 32 B x npulses x tiles of 32x32
- *    pixels + 8 B x pixels);
- *  - every call shares the array, so calls must not overlap on the GPU;
- *  - the first call on a device looks up the array and sets kernel
- *    attributes -- make it before any stream capture;
+ *    (roughly: 256 KiB of twiddle tables + 16 B x npulses x n_fft + 32 B x
+ *    npulses x tiles of 32x32 pixels + 8 B x pixels);
+ *  - every call shares the array and it keeps the last call's contents, so
+ *    calls that overlap on the GPU race: serialise them;
+ *  - the first call on a device looks up the array, sets kernel attributes
+ *    and fills the twiddle tables, then waits for `cuda_stream`; make it
+ *    before any stream capture.  That set-up is kept until the process
+ *    exits: after cudaDeviceReset the entry point must not be used again;
  *  - precision SARBP_PREC_COMPAT or SARBP_PREC_PRECISE only;
- *  - `status` (device int, may be NULL) receives the kernels' status bits
- *    (0 = fine; 1 = a pixel tile too spread out; 2 = non-finite geometry;
- *    8 = a bounded wait for a copy gave up).
+ *  - `status` (device int) receives the kernels' status bits (0 = fine;
+ *    1 = a pixel tile too spread out, left at zero; 2 = non-finite geometry;
+ *    8 = a bounded wait for a copy gave up).  It may be NULL, but then
+ *    those conditions go unreported: the call returns SARBP_OK and the image
+ *    may be wrong.
  * The array stays allocated on every GPU that loads the library until exit.
  */
 int sarbp_backprojection_noalloc(const sarbp_job *job, void *cuda_stream, int *status);
@@ -278,9 +399,19 @@ int sarbp_img_output_u8_device(sarbp_ctx *ctx, const double *dB, int nu,
                                int nv, double dB_min, double dB_max,
                                uint8_t *out);
 
+/* img_output_to_dB then img_output_u8 (sarbp.cpp:299-316) in one device
+ * pass that writes only the u8 image (no f64 dB image): a max|z| reduction,
+ * then the per-pixel grey levels.  The same conversion as the u8 output of a
+ * job (sarbp_job.out_u8).  Enqueued, not synchronised. */
+int sarbp_img_output_u8_from_img_device(sarbp_ctx *ctx, const double *img, int nu,
+                                        int nv, double dB_min, double dB_max,
+                                        uint8_t *out);
+
 /* ---- host helpers used by the CLI and the harness ---- */
 /* Taylor window (signal.h:14-51), f64 [num]. */
 int sarbp_taylor(int num, double S_L, double *out);
+/* The same with a SARBP_TAYLOR_* mode (no counterpart in the reference). */
+int sarbp_taylor_mode(int num, double S_L, int mode, double *out);
 /* nu/nv of img_plane_create (ImgPlane.cpp:20-28). */
 int sarbp_img_plane_dims(int nsamples, int npulses, int upsample, int *nu,
                          int *nv);

@@ -15,6 +15,7 @@ import numpy as np
 
 MODE_REF = 0
 MODE_FP64 = 1
+TAYLOR_FLOAT = 16  # mode flag: Taylor F_m denominator quotient in floating point
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libsarbp_oracle.so")
@@ -36,6 +37,7 @@ def lib():
             build()
         L = ctypes.CDLL(_LIB_PATH)
         L.orc_taylor.argtypes = [ctypes.c_int, ctypes.c_double, _dp]
+        L.orc_taylor_mode.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp]
         L.orc_linspace_f32.argtypes = [ctypes.c_float, ctypes.c_float, ctypes.c_int, _fp]
         L.orc_arange_f32.argtypes = [ctypes.c_float, ctypes.c_float, ctypes.c_int, _fp]
         L.orc_norm_f32.argtypes = [_fp, ctypes.c_int]
@@ -71,9 +73,11 @@ def max_threads():
     return lib().orc_max_threads()
 
 
-def taylor(num, s_l):
+def taylor(num, s_l, taylor_mode=0):
+    """Taylor window; taylor_mode 1 takes the F_m denominator quotient in
+    floating point (the float-division variant) instead of Int32."""
     out = np.empty(num, np.float64)
-    lib().orc_taylor(int(num), float(s_l), _ptr(out, ctypes.c_double))
+    lib().orc_taylor_mode(int(num), float(s_l), int(bool(taylor_mode)), _ptr(out, ctypes.c_double))
     return out
 
 
@@ -154,8 +158,11 @@ def fft_forward(x):
     return a
 
 
-def range_compress(phs, k_r, taylor_s_l, n_fft, mode=MODE_REF, nthreads=0):
-    """phs complex64 [P, S] -> Q complex128 [P, N_fft]."""
+def range_compress(phs, k_r, taylor_s_l, n_fft, mode=MODE_REF, nthreads=0, taylor_mode=0):
+    """phs complex64 [P, S] -> Q complex128 [P, N_fft]; taylor_mode 1 selects
+    the float-division Taylor window."""
+    if taylor_mode:
+        mode |= TAYLOR_FLOAT
     phs = np.ascontiguousarray(phs, np.complex64)
     P, S = phs.shape
     k_r = np.ascontiguousarray(k_r, np.float64)
@@ -195,8 +202,8 @@ def backproject(Q, S, delta_r, k_r, pos, r, nu, nv, out_idx=None, mode=MODE_REF,
 
 
 def backprojection(phs, k_r, taylor_s_l, n_fft, delta_r, pos, r, nu, nv, mode=MODE_REF,
-                   out_idx=None, nthreads=0):
-    Q = range_compress(phs, k_r, taylor_s_l, n_fft, mode, nthreads)
+                   out_idx=None, nthreads=0, taylor_mode=0):
+    Q = range_compress(phs, k_r, taylor_s_l, n_fft, mode, nthreads, taylor_mode)
     return backproject(Q, phs.shape[1], delta_r, k_r, pos, r, nu, nv, out_idx, mode, nthreads)
 
 

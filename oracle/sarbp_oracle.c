@@ -118,7 +118,13 @@ float orc_norm3d_f32(const float *p) {
  *  - xi = linspace(-0.5, 0.5, num) with no factor 2 inside the cosine
  *    (signal.h:27,45); the result is divided by its maximum (signal.h:48).
  */
-void orc_taylor(int num, double S_L, double *out) {
+void orc_taylor(int num, double S_L, double *out) { orc_taylor_mode(num, S_L, 0, out); }
+
+/* The same window with the F_m denominator quotient (m+1)^2/(r+1)^2 taken
+ * in f64 when float_den is non-zero (the float-division variant; the
+ * published RITSAR taylor() that signal.h restates divides in floating
+ * point). */
+void orc_taylor_mode(int num, double S_L, int float_den, double *out) {
     float p10 = powf(10.0f, (float)(S_L * (1.0 / 20)));
     float ach = logf(p10 + sqrtf(p10 * p10 - 1.0f)); /* acosh_f32 */
     double A = (1.0 / (double)M_PI) * (double)ach;
@@ -138,7 +144,8 @@ void orc_taylor(int num, double S_L, double *out) {
             fnum = fnum * ((double)sgn * (1.0 - (double)m1sq / sp2 / (A2 + rh * rh)));
             if (m != r) {
                 int r1sq = (r + 1) * (r + 1);
-                fden = fden * (1.0 - (double)floordiv(m1sq, r1sq));
+                double q = float_den ? (double)m1sq / (double)r1sq : (double)floordiv(m1sq, r1sq);
+                fden = fden * (1.0 - q);
             }
         }
         F[m] = fnum / fden;
@@ -310,8 +317,10 @@ int orc_range_compress(const float *phs, int S, int P, const double *k_r,
     if (S <= 0 || P <= 0 || N <= 0) return -1;
     double *wS = (double *)malloc(sizeof(double) * (size_t)S);
     double *wP = (double *)malloc(sizeof(double) * (size_t)P);
-    orc_taylor(S, (double)taylor_s_l, wS);
-    orc_taylor(P, (double)taylor_s_l, wP);
+    int float_den = (mode & ORC_TAYLOR_FLOAT) != 0;
+    mode &= ~ORC_TAYLOR_FLOAT;
+    orc_taylor_mode(S, (double)taylor_s_l, float_den, wS);
+    orc_taylor_mode(P, (double)taylor_s_l, float_den, wP);
     long long x_pad = floordiv((long long)N - S, 2);
     long long xm = N / 2 + N % 2;
     long long pm = P / 2 + P % 2;
@@ -477,6 +486,7 @@ int orc_backprojection(const float *phs, int S, int P, const double *k_r,
     double *Q = (double *)malloc(sizeof(double) * 2 * (size_t)P * (size_t)N);
     if (!Q) return -2;
     int rc = orc_range_compress(phs, S, P, k_r, taylor_s_l, N, mode, Q, nthreads);
+    mode &= ~ORC_TAYLOR_FLOAT;
     if (rc == 0)
         rc = orc_backproject(Q, P, N, S, delta_r, k_r, pos, r, nu, nv, NULL, 0,
                              mode, out_img, nthreads);

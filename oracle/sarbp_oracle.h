@@ -30,10 +30,15 @@ extern "C" {
 
 #define ORC_MODE_REF 0
 #define ORC_MODE_FP64 1
+/* flag or'ed into the mode of orc_range_compress / orc_backprojection: the
+ * Taylor window's F_m denominator quotient in floating point instead of the
+ * reference's Int32 division (see orc_taylor_mode) */
+#define ORC_TAYLOR_FLOAT 16
 
 /* ---- helper-level restatements (util.h, signal.h, img_plane.cpp) ---- */
 int orc_ip_upsample(int n);
 void orc_taylor(int num, double S_L, double *out);
+void orc_taylor_mode(int num, double S_L, int float_den, double *out);
 void orc_linspace_f32(float start, float stop, int num, float *out);
 void orc_linspace_f64(double start, double stop, int num, double *out);
 void orc_arange_f32(float start, float step, int n, float *out);

@@ -45,6 +45,22 @@ def test_taylor_matches_oracle(sb, oracle, known_answers):
         np.testing.assert_array_equal(sb.taylor(n, sl), oracle.taylor(n, sl))
 
 
+def test_taylor_float_mode_matches_oracle_and_is_defined_above_30_db(sb, oracle):
+    """TAYLOR_FLOAT (the F_m denominator quotient in floating point) equals
+    the oracle's float-division window at every level; the reference's
+    Int32-division window is only defined up to 30 dB."""
+    for n, sl in ((1999, 17), (424, 30), (1024, 31), (777, 35), (2000, 45)):
+        w = sb.taylor(n, sl, sb.TAYLOR_FLOAT)
+        np.testing.assert_array_equal(w, oracle.taylor(n, sl, taylor_mode=1))
+        assert np.all(np.isfinite(w)) and abs(w.max() - 1.0) < 1e-15
+    # both variants agree where no Int32 quotient rounds (n_bar <= 3)
+    np.testing.assert_array_equal(sb.taylor(500, 17, sb.TAYLOR_FLOAT), sb.taylor(500, 17))
+    # above 30 dB the reference's window is 0/0 somewhere
+    assert not np.all(np.isfinite(oracle.taylor(500, 31)))
+    with pytest.raises(sb.SarbpError):
+        sb.taylor(500, 20, 7)
+
+
 def test_img_plane_matches_fixture(sb, afrl_input, afrl_img_plane):
     ip = sb.img_plane_create(int(afrl_input["nsamples"][0]), int(afrl_input["npulses"][0]),
                              float(afrl_input["delta_r"][0]), afrl_input["R_c"])

@@ -103,7 +103,7 @@ def test_autotune_and_oracle(ctx, oracle, mixed_jobs):
         idx = rng.choice(j.nu * j.nv, size=min(2000, j.nu * j.nv), replace=False)
         want = oracle.backprojection(d["phs"], d["k_r"].astype(np.float32), d["taylor"], d["N_fft"],
                                      d["delta_r"], d["pos"].astype(np.float32), r, j.nu, j.nv,
-                                     out_idx=idx)
+                                     out_idx=idx, taylor_mode=d["taylor_mode"])
         got = j.image().ravel()[idx]
         assert rel_l2(got, want) < 1e-4, (j.nu, j.P, j.S)
 
@@ -127,3 +127,34 @@ def test_u8_stage_equals_reference_formula(ctx, oracle, mixed_jobs, lo, hi):
     d = mixed_jobs[0].data.get("db", (-40.0, 0.0))
     for j in mixed_jobs:
         j.job.dB_min, j.job.dB_max = d
+
+
+def test_taylor_above_30_db_float_window_matches_oracle(ctx, sb, oracle):
+    """Side-lobe levels 31-35 dB (where the reference's Int32-division window
+    is undefined) run with the float-quotient window (TAYLOR_FLOAT) and match
+    the oracle's float-division window at reference precision; the same jobs
+    with the reference's window are rejected."""
+    import torch
+    from sarbp_b200 import synth
+    from sarbp_b200.batch import DeviceJob
+    cfgs = synth.batch_jobs(njobs=5, seed=17, sizes=(128, 256), pulses=(150, 400), samples=(256, 512),
+                            taylors=(31, 35))
+    jobs = [DeviceJob(c, torch, "cuda") for c in cfgs]
+    assert all(j.data["taylor_mode"] == sb.TAYLOR_FLOAT for j in jobs)
+    ctx.run_jobs([j.job for j in jobs])
+    ctx.synchronize()
+    rng = np.random.default_rng(8)
+    for j in jobs:
+        d = j.data
+        r = oracle.pixel_locs(d["u"], d["v"], d["u_hat"], d["v_hat"])
+        idx = rng.choice(j.nu * j.nv, size=1500, replace=False)
+        want = oracle.backprojection(d["phs"], d["k_r"].astype(np.float32), d["taylor"], d["N_fft"],
+                                     d["delta_r"], d["pos"].astype(np.float32), r, j.nu, j.nv,
+                                     out_idx=idx, taylor_mode=1)
+        assert rel_l2(j.image().ravel()[idx], want) < 1e-4, (d["taylor"], j.nu, j.P)
+    ref_job = jobs[0].job
+    ref_job.taylor_mode = sb.TAYLOR_REF
+    with pytest.raises(sb.SarbpError) as e:
+        ctx.run_jobs([ref_job])
+    assert e.value.code == sb.ERR_INVALID and b"30 dB" in str(e.value).encode()
+    ref_job.taylor_mode = sb.TAYLOR_FLOAT

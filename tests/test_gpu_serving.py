@@ -79,7 +79,8 @@ def test_served_vs_fp64_sample(ctx, sb, oracle, pool):
         r = oracle.pixel_locs(d["u"], d["v"], d["u_hat"], d["v_hat"])
         idx = rng.choice(hj.nu * hj.nv, 1500, replace=False)
         ref = oracle.backprojection(d["phs"], d["k_r"], d["taylor"], d["N_fft"], d["delta_r"], d["pos"], r,
-                                    hj.nu, hj.nv, mode=oracle.MODE_FP64, out_idx=idx)
+                                    hj.nu, hj.nv, mode=oracle.MODE_FP64, out_idx=idx,
+                                    taylor_mode=d["taylor_mode"])
         e = rel_l2(out.ravel()[idx], ref)
         print("served request %d (%dx%d, %d pulses): rel-L2 vs FP64 %.2e" % (k, hj.nu, hj.nv, hj.P, e))
         assert e < 1e-3
@@ -118,5 +119,57 @@ def test_wait_times_out_while_queued(ctx, sb, pool):
         assert time.perf_counter() - t0 < 1.0
         for r in rids:
             assert srv.wait(r, 60.0) == 0
+    finally:
+        srv.close()
+
+
+def test_registered_aperture_skips_upload_and_range_compression(ctx, sb, pool):
+    """A phase history registered once stays resident: requests on it give
+    the same image, bit for bit, as requests that bring the phase history,
+    the server copies only their image-plane axes, and no pulse is
+    range-compressed after the registration."""
+    from sarbp_b200 import _lib
+    srv = sb.Server(ctx, hbm_cap_bytes=8e9, lanes=2, max_batch=8, precision=sb.PREC_PRECISE)
+    try:
+        hj = pool[1]
+        rid, direct = _submit(srv, hj, sb.PREC_PRECISE)
+        assert srv.wait(rid, 60.0) == 0
+        base_use = srv.stats()["in_use_bytes"]
+        dummy = hj.new_outputs()[0]
+        ap = srv.register(hj.job(dummy, precision=sb.PREC_PRECISE))
+        c0 = srv.counters()
+        assert srv.stats()["in_use_bytes"] > base_use  # resident profiles are charged
+        outs = []
+        for _ in range(6):
+            out = hj.new_outputs()[0]
+            outs.append((srv.submit_on(ap, hj.job(out), keep=out), out))
+        for r, out in outs:
+            assert srv.wait(r, 60.0) == 0
+            assert np.array_equal(out, direct)
+        c1 = srv.counters()
+        assert c1["rc_pulses"] == c0["rc_pulses"]
+        assert c1["resident_requests"] - c0["resident_requests"] == 6
+        assert c1["h2d_bytes"] - c0["h2d_bytes"] == 6 * (hj.u.nbytes + hj.v.nbytes)
+        with pytest.raises(sb.SarbpError) as e:
+            srv.submit_on(ap + 100, hj.job(dummy))
+        assert e.value.code == _lib.ERR_INVALID
+        srv.unregister(ap)
+        assert srv.stats()["in_use_bytes"] == base_use
+        with pytest.raises(sb.SarbpError):
+            srv.unregister(ap)
+    finally:
+        srv.close()
+
+
+def test_register_over_budget_is_an_admission_error(ctx, sb):
+    from sarbp_b200 import _lib, synth
+    from sarbp_b200.batch import HostJob
+    srv = sb.Server(ctx, hbm_cap_bytes=64e6, lanes=1, max_batch=2, precision=sb.PREC_COMPAT)
+    try:
+        big = HostJob(synth.batch_jobs(njobs=1, seed=4, sizes=(256,), pulses=(1900, 2000), samples=(1024,))[0])
+        with pytest.raises(sb.SarbpError) as e:
+            srv.register(big.job(big.new_outputs()[0]))
+        assert e.value.code == _lib.ERR_ADMISSION
+        assert srv.stats()["in_use_bytes"] == 0
     finally:
         srv.close()
