@@ -166,11 +166,54 @@ def cpu_baseline_sample(data, seconds, nthreads=0):
                 cores=O.max_threads())
 
 
+def host_info():
+    """The host the CPU figures were taken on: nproc, OMP_NUM_THREADS, model."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count(), "omp_num_threads": os.environ.get("OMP_NUM_THREADS"), "cpu_model": model}
+
+
+def oracle_workload(name, seed, with_r=True):
+    """The named configuration's workload generated by the oracle alone (the
+    same data as sarbp_b200.synth.make, without the product library)."""
+    from sarbp_b200.synth import CONFIGS, scene  # parameters only: loads no native code
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cfg = CONFIGS[name]
+    d = O.make_workload(cfg, scene(cfg["nscat"], cfg["half"], cfg["clutter"], seed), seed, with_r=with_r)
+    d["name"] = name
+    return d
+
+
+def cpu_whole_image(name="plain_small", seed=2):
+    """One whole image of `name` on the CPU oracle (reference precision, all
+    host threads): range compression of all pulses and every pixel."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    d = oracle_workload(name, seed)
+    k32 = d["k_r"].astype(np.float32).astype(np.float64)
+    pos32 = d["pos"].astype(np.float32).astype(np.float64)
+    t0 = time.perf_counter()
+    O.backprojection(d["phs"], k32, d["taylor"], d["N_fft"], d["delta_r"], pos32, d["r"], d["nu"], d["nv"],
+                     mode=O.MODE_REF)
+    t = time.perf_counter() - t0
+    return {"workload": "%s: %dx%d image, %d pulses x %d samples, N_fft %d" % (
+                name, d["nu"], d["nv"], d["P"], d["S"], d["N_fft"]),
+            "seconds": t, "value": d["nu"] * d["nv"] * d["P"] / t / 1e9, "unit": "Gpixel*pulses/s",
+            "cores": O.max_threads()}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    from sarbp_b200 import synth
-    data = synth.make(args.config, seed=2)
+    data = oracle_workload(args.config, 2)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     O.lib()
@@ -212,11 +255,11 @@ def run_reference(args, rank, world):
         "data": "synthetic (seeded, plain_large shapes)",
         "config": config_block(data, world),
         "cpu_baseline": {"value": value, "unit": "Gpixel*pulses/s", "cores": cores, "kind": "port",
-                         "sample": sample},
+                         "sample": sample, "host": host_info(), "whole_image": cpu_whole_image()},
         "e2e": {"value": value, "unit": "Gpixel*pulses/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
-        "note": "reference CPU schedule restated in C (oracle/sarbp_oracle.c); the reference "
-                "itself needs Halide/FFTW/cnpy, which are not installable here",
+        "note": "reference CPU schedule restated in C (oracle/sarbp_oracle.c), inputs from the oracle's "
+                "own generator; the reference itself needs Halide/FFTW/cnpy, which are not installable here",
     }
     print(json.dumps(out), flush=True)
 
@@ -419,7 +462,8 @@ def run_ours(args, rank, world, local_rank):
                                "sample": "%d random pixels x %d pulses (reference-precision C oracle, "
                                          "%d threads, %.1f s; range compression of all pulses "
                                          "charged pro rata)" % (cb["n_pix"], P, cb["cores"],
-                                                                cb["seconds"])}
+                                                                cb["seconds"]),
+                               "host": host_info(), "whole_image": cpu_whole_image()}
     if world == 1 and args.config == "plain_large" and not args.no_extras:
         # the rest of the headline metric: the batched form (ratio to the
         # plain single image above) and the serving loop (p50/p99 and the

@@ -177,12 +177,14 @@ int run(int argc, char **argv) {
 
     std::vector<double> img((size_t)nu * nv * 2);
     for (unsigned i = 1; i <= num_iters; ++i) {
-        std::cout << "(" << i << ") backprojection start " << std::endl;
+        // the reference's progress lines verbatim (sarbp.cpp:275,279), so
+        // that tools reading its output keep working
+        std::cout << "(" << i << ") Halide backprojection start " << std::endl;
         t0 = steady_clock::now();
         rv = sarbp_backprojection_plane(ctx, pd.phs.data(), pd.nsamples, pd.npulses, pd.k_r.data(), taylor,
                                         N_fft, pd.delta_r, u.data(), nu, v.data(), nv, u_hat, v_hat,
                                         pd.pos.data(), img.data(), nullptr);
-        std::cout << "(" << i << ") backprojection returned " << rv << " in " << ms_since(t0) << " ms"
+        std::cout << "(" << i << ") Halide backprojection returned " << rv << " in " << ms_since(t0) << " ms"
                   << std::endl;
         if (rv != 0) {
             std::cerr << sarbp_last_error() << std::endl;
@@ -191,20 +193,20 @@ int run(int argc, char **argv) {
     }
 
     std::vector<double> dB((size_t)nu * nv);
-    std::cout << "dB conversion start" << std::endl;
+    std::cout << "Halide dB conversion start" << std::endl;
     t0 = steady_clock::now();
     rv = sarbp_img_output_to_dB(ctx, img.data(), nu, nv, dB.data());
-    std::cout << "dB conversion returned " << rv << " in " << ms_since(t0) << " ms" << std::endl;
+    std::cout << "Halide dB conversion returned " << rv << " in " << ms_since(t0) << " ms" << std::endl;
     if (rv != 0) {
         std::cerr << sarbp_last_error() << std::endl;
         return rv;
     }
 
     std::vector<uint8_t> u8((size_t)nu * nv);
-    std::cout << "PNG production start" << std::endl;
+    std::cout << "Halide PNG production start" << std::endl;
     t0 = steady_clock::now();
     rv = sarbp_img_output_u8(ctx, dB.data(), nu, nv, dB_min, dB_max, u8.data());
-    std::cout << "PNG production returned " << rv << " in " << ms_since(t0) << " ms" << std::endl;
+    std::cout << "Halide PNG production returned " << rv << " in " << ms_since(t0) << " ms" << std::endl;
     if (rv != 0) {
         std::cerr << sarbp_last_error() << std::endl;
         return rv;

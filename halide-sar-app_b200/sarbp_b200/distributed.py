@@ -10,6 +10,12 @@ crosses between ranks before the gather.  Output row y holds pixel row
 nv - 1 - y (the reference's row flip, backprojection.cpp:130), so the block
 [y0, y1) is the job over pixel rows [nv - y1, nv - y0), whose own flipped
 rows are exactly that block in order.
+
+The data path stays on the device: each rank's kernels write its block
+straight into its slice of an equal-size send buffer in device memory, the
+blocks are gathered device to device (NCCL gather; with gloo, on the CPU,
+the same buffers live in host memory), and the destination rank copies the
+assembled image to the host once.
 """
 import numpy as np
 
@@ -26,56 +32,109 @@ def pixel_rows(nv, y0, y1):
     return nv - y1, nv - y0
 
 
-def cuda_compute(ctx, phs, k_r, taylor_s_l, n_fft, delta_r, u, pos, **kw):
-    """compute(v_rows, r_rows) on this rank's GPU through the host entry
-    point (Context.backprojection_cuda)."""
-    def compute(v_rows, r_rows):
-        return ctx.backprojection_cuda(phs, k_r, taylor_s_l, n_fft, delta_r, u, v_rows, pos, r_rows, **kw)
-    return compute
+class DeviceCompute:
+    """compute(a, b, out) on this rank's GPU: forms pixel rows [a, b) of the
+    job into `out`, a float64 CUDA tensor [b - a, nu, 2] (complex128 rows in
+    output order), through the device entry point.  The phase history, k_r,
+    antenna positions and image-plane axes (or pixel positions r, SoA
+    [3, nu * nv]) are uploaded once; the context launches on torch's current
+    stream, so the gather that follows is ordered after the kernels."""
+
+    def __init__(self, ctx, phs, k_r, taylor_s_l, n_fft, delta_r, u, v, pos, u_hat=None, v_hat=None, r=None,
+                 precision=None, taylor_mode=0):
+        import torch
+        import sarbp_b200 as sb
+        self.sb, self.torch, self.ctx = sb, torch, ctx
+        dev = torch.device("cuda", torch.cuda.current_device())
+        to = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dt)).to(dev)
+        phs = np.ascontiguousarray(phs, np.complex64)
+        self.P, self.S = phs.shape
+        self.phs = to(phs.view(np.float32), np.float32)
+        wide = np.asarray(pos).dtype == np.float64
+        self.precision = (sb.PREC_PRECISE if wide else sb.PREC_COMPAT) if precision is None else precision
+        self.k32, self.p32 = to(k_r, np.float32), to(pos, np.float32)
+        self.k64, self.p64 = to(k_r, np.float64), to(pos, np.float64)
+        self.u, self.v = to(u, np.float64), to(v, np.float64)
+        self.nu, self.nv = len(u), len(v)
+        self.r = to(r, np.float64).reshape(3, self.nv, self.nu) if r is not None else None
+        self.u_hat = (0.0, 0.0, 0.0) if u_hat is None else tuple(u_hat)
+        self.v_hat = (0.0, 0.0, 0.0) if v_hat is None else tuple(v_hat)
+        self.taylor, self.n_fft, self.delta_r, self.taylor_mode = taylor_s_l, n_fft, delta_r, taylor_mode
+        ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+
+    def __call__(self, a, b, out):
+        sb = self.sb
+        rows = b - a
+        kw = {}
+        keep = None
+        if self.r is not None:
+            keep = self.r[:, a:b, :].contiguous()  # rows a..b of each coordinate
+            kw["r"] = keep.data_ptr()
+        else:
+            kw.update(u=self.u.data_ptr(), v=self.v.data_ptr() + 8 * a, u_hat=self.u_hat, v_hat=self.v_hat)
+        job = sb.make_job(self.S, self.P, self.n_fft, self.taylor, self.nu, rows, self.delta_r,
+                          self.phs.data_ptr(), self.k32.data_ptr(), self.p32.data_ptr(), out.data_ptr(),
+                          k_r64=self.k64.data_ptr(), pos64=self.p64.data_ptr(), precision=self.precision,
+                          taylor_mode=self.taylor_mode, **kw)
+        self.ctx.run_jobs([job])
+        self.ctx.synchronize()  # raises on a kernel status error; `keep` is read by then
 
 
-def cuda_compute_plane(ctx, phs, k_r, taylor_s_l, n_fft, delta_r, u, u_hat, v_hat, pos, **kw):
-    """compute(v_rows, None) on this rank's GPU from the image-plane axes
-    (Context.backprojection_plane): no pixel-position array at all."""
-    def compute(v_rows, r_rows):
-        return ctx.backprojection_plane(phs, k_r, taylor_s_l, n_fft, delta_r, u, v_rows, u_hat, v_hat, pos, **kw)
-    return compute
+def form_block(compute, nu, nv, world, rank, device="cpu"):
+    """This rank's equal-size send buffer (float64 [ceil(nv/world), nu, 2]
+    on `device`) with its block of output rows formed by compute(a, b, out)
+    into the leading rows."""
+    import torch
+    blocks = output_row_blocks(nv, world)
+    y0, y1 = blocks[rank]
+    step = blocks[0][1] - blocks[0][0]
+    send = torch.zeros((step, nu, 2), dtype=torch.float64, device=device)
+    if y1 > y0:
+        a, b = pixel_rows(nv, y0, y1)
+        compute(a, b, send[: y1 - y0])
+    return send
 
 
-def distributed_backprojection(compute, u, v, r, group=None, dst=0):
-    """Forms this rank's block of output rows with compute(v_rows, r_rows)
-    (-> complex128 [rows, nu]) and gathers the blocks on rank `dst`, which
-    returns the whole image complex128 [nv, nu]; the other ranks return None.
-    r is SoA [3, nu * nv] (pixel_locs) or None when compute forms the
-    positions itself (then r_rows is None)."""
+def assemble(gathered, nu, nv):
+    """The image complex128 [nv, nu] (host) from the ranks' send buffers in
+    rank order: the blocks are joined where they lie, then copied once."""
+    import torch
+    world = len(gathered)
+    parts = [g[: y1 - y0] for g, (y0, y1) in zip(gathered, output_row_blocks(nv, world)) if y1 > y0]
+    full = torch.cat(parts, 0)
+    return np.ascontiguousarray(full.cpu().numpy()).view(np.complex128)[..., 0]
+
+
+def distributed_backprojection(compute, nu, nv, group=None, dst=0):
+    """Forms this rank's block of output rows with compute(a, b, out) (pixel
+    rows [a, b) into the float64 tensor out [b - a, nu, 2], on the CUDA
+    device for an NCCL group, in host memory for gloo) and gathers the
+    blocks on rank `dst`, which returns the whole image complex128 [nv, nu];
+    the other ranks return None."""
     import torch
     import torch.distributed as dist
     world = dist.get_world_size(group)
     rank = dist.get_rank(group)
-    nu, nv = len(u), len(v)
-    blocks = output_row_blocks(nv, world)
-    y0, y1 = blocks[rank]
-    a, b = pixel_rows(nv, y0, y1)
-    rows = y1 - y0
-    if rows > 0:
-        r_rows = None if r is None else np.ascontiguousarray(
-            np.asarray(r).reshape(3, nv, nu)[:, a:b, :].reshape(3, rows * nu))
-        img = np.ascontiguousarray(compute(np.asarray(v)[a:b], r_rows), np.complex128)
-    else:
-        img = np.zeros((0, nu), np.complex128)
-    # equal-size blocks for the collective: pad to the first block's rows
-    step = blocks[0][1] - blocks[0][0]
-    dev = torch.device("cuda", torch.cuda.current_device()) \
+    device = torch.device("cuda", torch.cuda.current_device()) \
         if dist.get_backend(group) == "nccl" else torch.device("cpu")
-    send = torch.zeros((step, nu, 2), dtype=torch.float64, device=dev)
-    if rows:
-        send[:rows] = torch.from_numpy(img.view(np.float64).reshape(rows, nu, 2)).to(dev)
+    send = form_block(compute, nu, nv, world, rank, device)
     gather = [torch.empty_like(send) for _ in range(world)] if rank == dst else None
     dist.gather(send, gather_list=gather, dst=dst, group=group)
     if rank != dst:
         return None
-    out = np.empty((nv, nu), np.complex128)
-    for k, (g0, g1) in enumerate(blocks):
-        if g1 > g0:
-            out[g0:g1] = gather[k][: g1 - g0].cpu().numpy().view(np.complex128)[..., 0]
-    return out
+    return assemble(gather, nu, nv)
+
+
+def oracle_compute(backprojection, phs, k_r, taylor_s_l, n_fft, delta_r, u, v, pos, r, **kw):
+    """compute(a, b, out) from a CPU backprojection function with the
+    oracle's signature (phs, k_r, taylor, n_fft, delta_r, pos, r, nu, nv):
+    pixel rows [a, b) of r (SoA [3, nu * nv]) written into a host tensor."""
+    nu, nv = len(u), len(v)
+    r3 = np.asarray(r).reshape(3, nv, nu)
+
+    def compute(a, b, out):
+        import torch
+        rr = np.ascontiguousarray(r3[:, a:b, :].reshape(3, (b - a) * nu))
+        img = backprojection(phs, k_r, taylor_s_l, n_fft, delta_r, pos, rr, nu, b - a, **kw)
+        out.copy_(torch.from_numpy(np.ascontiguousarray(img).view(np.float64).reshape(b - a, nu, 2)))
+    return compute

@@ -61,6 +61,9 @@ def lib():
         L.orc_img_output_u8.argtypes = [_dp, ctypes.c_longlong, ctypes.c_double,
                                         ctypes.c_double, ctypes.POINTER(ctypes.c_ubyte)]
         L.orc_max_threads.restype = ctypes.c_int
+        L.orc_synth_phase_history.argtypes = [
+            ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+            ctypes.c_double, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong, _fp, _dp, _dp, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -220,4 +223,47 @@ def img_output_u8(dB, dB_min, dB_max):
     out = np.empty(dB.shape, np.uint8)
     lib().orc_img_output_u8(_ptr(dB, ctypes.c_double), dB.size, float(dB_min), float(dB_max),
                             _ptr(out, ctypes.c_ubyte))
+    return out
+
+
+C_LIGHT = 299792458.0
+
+
+def synth_phase_history(S, P, f0, df, R0, dep, span, scat, snr_db, seed, nthreads=0):
+    """Seeded synthetic phase history (orc_synth_phase_history): returns
+    (phs complex64 [P, S], pos f64 [P, 3], k_r f64 [S])."""
+    scat = np.ascontiguousarray(scat, np.float64)
+    phs = np.empty((P, S), np.complex64)
+    pos = np.empty((P, 3), np.float64)
+    k_r = np.empty(S, np.float64)
+    rc = lib().orc_synth_phase_history(int(S), int(P), float(f0), float(df), float(R0), float(dep), float(span),
+                                       _ptr(scat, ctypes.c_double), int(scat.shape[0]), float(snr_db),
+                                       int(seed), phs.view(np.float32).ctypes.data_as(_fp),
+                                       _ptr(pos, ctypes.c_double), _ptr(k_r, ctypes.c_double), int(nthreads))
+    if rc:
+        raise ValueError("orc_synth_phase_history failed: %d" % rc)
+    return phs, pos, k_r
+
+
+def make_workload(cfg, scat, seed, with_r=True, nthreads=0):
+    """A benchmark workload from its configuration dict (P, S, f0, df, R0,
+    dep, span, snr, n, extent, taylor, upsample, db) and scene, with the
+    oracle alone: phase history, positions, k_r, delta_r, N_fft, and a
+    square n x n image plane over `extent` metres whose axes come from the
+    reference's image-plane construction with R_c the mid-aperture position
+    (ImgPlane.cpp:16-63), pixel positions SoA [3, n*n]."""
+    S, P = cfg["S"], cfg["P"]
+    phs, pos, k_r = synth_phase_history(S, P, cfg["f0"], cfg["df"], cfg["R0"], cfg["dep"], cfg["span"], scat,
+                                        cfg["snr"], seed, nthreads)
+    delta_r = C_LIGHT / (2.0 * S * cfg["df"])
+    ip = img_plane(S, P, delta_r, pos[P // 2].astype(np.float32), pixel_locs=False)
+    n = cfg["n"]
+    d = cfg["extent"] / n
+    u = (np.arange(n) - n // 2) * d
+    v = (np.arange(n) - n // 2) * d
+    out = dict(cfg=cfg, phs=phs, pos=pos, k_r=k_r, delta_r=delta_r, S=S, P=P, nu=n, nv=n, u=u, v=v,
+               u_hat=ip["u_hat"], v_hat=ip["v_hat"], taylor=cfg["taylor"], db=cfg["db"],
+               N_fft=int(2 ** (int(np.log2(S * cfg["upsample"])) + 1)))
+    if with_r:
+        out["r"] = pixel_locs(u, v, ip["u_hat"], ip["v_hat"])
     return out

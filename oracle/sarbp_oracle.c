@@ -525,3 +525,101 @@ void orc_img_output_u8(const double *dB, long long npix, double dB_min,
         out[i] = (unsigned char)n;
     }
 }
+
+/*
+ * Seeded synthetic stepped-frequency phase history for the CPU reference
+ * arm of the benchmark (it stands in for the reference's AFRL / Sandia
+ * inputs at the configurations' sizes): for pulse p at pos_p (a circular
+ * arc of P positions at slant range R0, depression dep_deg, azimuth span
+ * span_deg) and scatterer i (x, y, z, Re a, Im a),
+ *     S(f_k, p) = sum_i a_i exp(+j (4 pi f_k / c)(|pos_p| - |pos_p - x_i|))
+ * plus complex Gaussian noise at snr_db (none at 300 dB and above) from a
+ * counter-based hash of (seed, sample index).  The frequency ramp advances
+ * by a complex rotation and is re-seeded every 32 samples.  The same
+ * formulas, in the same order, as the product library's generator, so both
+ * arms of the benchmark see the same data.
+ */
+static unsigned long long orc_mix64(unsigned long long z) {
+    z += 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+static double orc_unit(unsigned long long h) { return ((double)(h >> 11) + 0.5) * (1.0 / 9007199254740992.0); }
+
+int orc_synth_phase_history(int S, int P, double f0, double df, double R0, double dep_deg,
+                            double span_deg, const double *scat, int nscat, double snr_db,
+                            unsigned long long seed, float *phs, double *pos, double *k_r,
+                            int nthreads) {
+    const double c = 299792458.0, pi = 3.14159265358979323846;
+    if (S < 1 || P < 1 || !phs || !pos || !k_r || nscat < 0 || (nscat > 0 && !scat)) return -1;
+    const double dep = dep_deg * pi / 180.0, span = span_deg * pi / 180.0;
+    for (int k = 0; k < S; k++) k_r[k] = 4.0 * pi * (f0 + df * k) / c;
+    for (int p = 0; p < P; p++) {
+        double phi = (P > 1 ? ((double)p / (P - 1) - 0.5) : 0.0) * span;
+        pos[3 * p] = R0 * cos(dep) * cos(phi);
+        pos[3 * p + 1] = R0 * cos(dep) * sin(phi);
+        pos[3 * p + 2] = R0 * sin(dep);
+    }
+    const double dk = 4.0 * pi * df / c;
+    double *acc = (double *)calloc((size_t)P * S * 2, sizeof(double));
+    double *pw = (double *)calloc((size_t)P, sizeof(double));
+    if (!acc || !pw) {
+        free(acc);
+        free(pw);
+        return -2;
+    }
+    set_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int p = 0; p < P; p++) {
+        const double *pp = pos + 3 * p;
+        const double np = sqrt(pp[0] * pp[0] + pp[1] * pp[1] + pp[2] * pp[2]);
+        double *a = acc + (size_t)p * S * 2;
+        for (int i = 0; i < nscat; i++) {
+            const double *s = scat + 5 * i;
+            const double ex = pp[0] - s[0], ey = pp[1] - s[1], ez = pp[2] - s[2];
+            const double D = np - sqrt(ex * ex + ey * ey + ez * ez);
+            const double rr = cos(dk * D), ri = sin(dk * D);
+            double zr = 0, zi = 0;
+            for (int k = 0; k < S; k++) {
+                if ((k & 31) == 0) {
+                    const double ph = k_r[k] * D;
+                    zr = cos(ph);
+                    zi = sin(ph);
+                } else {
+                    const double tr = zr * rr - zi * ri;
+                    zi = zr * ri + zi * rr;
+                    zr = tr;
+                }
+                a[2 * k] += s[3] * zr - s[4] * zi;
+                a[2 * k + 1] += s[3] * zi + s[4] * zr;
+            }
+        }
+        double sp = 0;
+        for (int k = 0; k < S; k++) sp += a[2 * k] * a[2 * k] + a[2 * k + 1] * a[2 * k + 1];
+        pw[p] = sp;
+    }
+    double total = 0;
+    for (int p = 0; p < P; p++) total += pw[p];
+    const double mean_pw = total / ((double)P * S);
+    const double sigma = snr_db < 300 ? sqrt(mean_pw / pow(10.0, snr_db / 10.0) / 2.0) : 0.0;
+#pragma omp parallel for schedule(static)
+    for (int p = 0; p < P; p++) {
+        for (int k = 0; k < S; k++) {
+            const size_t idx = (size_t)p * S + k;
+            double nr = 0, ni = 0;
+            if (sigma > 0) {
+                const double u1 = orc_unit(orc_mix64(seed ^ orc_mix64(2 * idx)));
+                const double u2 = orc_unit(orc_mix64(seed ^ orc_mix64(2 * idx + 1)));
+                const double rad = sqrt(-2.0 * log(u1));
+                nr = sigma * rad * cos(2 * pi * u2);
+                ni = sigma * rad * sin(2 * pi * u2);
+            }
+            phs[2 * idx] = (float)(acc[2 * idx] + nr);
+            phs[2 * idx + 1] = (float)(acc[2 * idx + 1] + ni);
+        }
+    }
+    free(acc);
+    free(pw);
+    return 0;
+}

@@ -98,6 +98,14 @@ void orc_img_output_u8(const double *dB, long long npix, double dB_min,
 
 int orc_max_threads(void);
 
+/* Seeded synthetic phase history (the benchmark's CPU arm generates its
+ * inputs with this, without the product library): phs complex64 [P][S],
+ * pos f64 [P][3], k_r f64 [S]; scat is [nscat][5] (x, y, z, Re a, Im a). */
+int orc_synth_phase_history(int S, int P, double f0, double df, double R0, double dep_deg,
+                            double span_deg, const double *scat, int nscat, double snr_db,
+                            unsigned long long seed, float *phs, double *pos, double *k_r,
+                            int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,7 +1,7 @@
 """Regenerates the golden fixtures in this folder from the reference checkout.
 
-Run in a container that has the reference at REF (default /root/reference):
-    python tests/golden/make_golden.py [REF]
+Run where the reference checkout is readable, passing its directory:
+    python tests/golden/make_golden.py REF      (or SARBP_REFERENCE=REF)
 
 Writes
   reference_known_answers.json  known-answer values of the reference's own
@@ -85,7 +85,10 @@ def known_answers(ref):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    # the reference checkout: the first argument, else $SARBP_REFERENCE
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SARBP_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py REFERENCE_DIR (or set SARBP_REFERENCE)")
     ka = known_answers(ref)
     with open(os.path.join(HERE, "reference_known_answers.json"), "w") as f:
         json.dump(ka, f, indent=1)

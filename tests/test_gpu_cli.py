@@ -78,7 +78,10 @@ def _cli(d, out_png):
 def test_cli_png_matches_oracle(tmp_path, afrl_input, afrl_reference):
     d = write_platform(str(tmp_path / "afrl"), afrl_input)
     out = _cli(d, str(tmp_path / "afrl.png"))
-    assert "(2) backprojection returned 0" in out and "Wrote" in out
+    # the reference's progress lines, verbatim (sarbp.cpp:275-326)
+    for line in ("(1) Halide backprojection start", "(2) Halide backprojection returned 0",
+                 "Halide dB conversion returned 0", "Halide PNG production returned 0", "Wrote "):
+        assert line in out, line
     got = read_png_gray8(str(tmp_path / "afrl.png"))
     ref = afrl_reference["u8"]
     assert got.shape == ref.shape == (512, 512)
@@ -138,23 +141,28 @@ def test_halide_shim_matches_c_abi(ctx, afrl_input, afrl_reference):
     assert np.array_equal(u8.arr, ctx.img_output_u8(dB.arr, DB_MIN, DB_MAX))
 
 
-def test_row_blocks_on_gpu_reassemble_the_image(ctx, afrl_input, afrl_reference):
+@pytest.mark.parametrize("form", ["r", "plane"])
+def test_row_blocks_on_gpu_reassemble_the_image(ctx, afrl_input, afrl_reference, form):
     """The per-rank work of the distributed mode (sarbp_b200.distributed),
-    run block by block on this GPU: three uneven blocks of output rows, each
-    formed as its own job, reassemble the whole image.  Block edges that do
-    not fall on 32-row tile edges give tiles with other centres, so the
-    match is to rounding (relative L2 < 1e-5), and to the oracle within the
-    compat tolerance."""
-    from sarbp_b200.distributed import cuda_compute, output_row_blocks, pixel_rows
+    run rank by rank on this GPU: each of three ranks' kernels write its
+    block of output rows straight into its device send buffer
+    (DeviceCompute, form_block), and the buffers assembled in rank order (as
+    rank 0 does after the NCCL gather) give the whole image.  Block edges
+    that do not fall on 32-row tile edges give tiles with other centres, so
+    the match is to rounding (relative L2 < 1e-5), and to the oracle within
+    the compat tolerance.  Pixel positions as the r array and as the
+    image-plane axes."""
+    import torch
+    from sarbp_b200.distributed import DeviceCompute, assemble, form_block
     pd, R = afrl_input, afrl_reference
     ip = R["ip"]
     nu, nv = ip["nu"], ip["nv"]
-    compute = cuda_compute(ctx, pd["phs"], pd["k_r"], TAYLOR, R["n_fft"], R["dr"], ip["u"], pd["pos"])
-    r3 = ip["pixel_locs"].reshape(3, nv, nu)
-    out = np.empty((nv, nu), np.complex128)
-    for y0, y1 in output_row_blocks(nv, 3):
-        a, b = pixel_rows(nv, y0, y1)
-        out[y0:y1] = compute(ip["v"][a:b], np.ascontiguousarray(r3[:, a:b, :].reshape(3, -1)))
-    whole = compute(ip["v"], ip["pixel_locs"])
+    kw = dict(r=ip["pixel_locs"]) if form == "r" else dict(u_hat=ip["u_hat"], v_hat=ip["v_hat"])
+    compute = DeviceCompute(ctx, pd["phs"], pd["k_r"], TAYLOR, R["n_fft"], R["dr"], ip["u"], ip["v"], pd["pos"],
+                            **kw)
+    sends = [form_block(compute, nu, nv, 3, k, device="cuda") for k in range(3)]
+    assert all(s.is_cuda for s in sends)
+    out = assemble(sends, nu, nv)
+    whole = assemble([form_block(compute, nu, nv, 1, 0, device="cuda")], nu, nv)
     assert rel_l2(out, whole) < 1e-5
     assert rel_l2(out, R["img"]) < 1e-4

@@ -165,3 +165,16 @@ def test_db_u8_semantics(oracle):
     u8 = oracle.img_output_u8(dB, -30.0, 0.0)
     assert u8[0, 0] == 255 and u8[0, 2] == 0 and u8.dtype == np.uint8
     assert u8[0, 1] == int((10 * np.log10(0.1) + 30) / 30 * 255)
+
+
+def test_oracle_generator_equals_the_library_generator(oracle, sb):
+    """The benchmark's CPU arm builds its inputs with the oracle's generator
+    (no product code in that arm): the same phase history, positions, k_r
+    and pixel positions, bit for bit, as the product library's generator."""
+    from sarbp_b200 import synth
+    cfg = dict(synth.CONFIGS["plain_small"], P=97, S=130, n=48, nscat=7, clutter=3)
+    d = synth.make("plain_small", seed=4, overrides=cfg)
+    w = oracle.make_workload(cfg, synth.scene(cfg["nscat"], cfg["half"], cfg["clutter"], 4), 4)
+    for k in ("phs", "pos", "k_r", "u", "v", "u_hat", "v_hat", "r"):
+        assert np.array_equal(d[k], w[k]), k
+    assert d["delta_r"] == w["delta_r"] and d["N_fft"] == w["N_fft"]
