@@ -265,6 +265,7 @@ int sarbp_ctx_destroy(sarbp_ctx *ctx) {
     ctx->runner.reset();
     ctx->io.release();
     ctx->out_aux.release();
+    ctx->resize_buf.release();
     ctx->dev.release();
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     for (cudaStream_t sp : {ctx->copy_in, ctx->aux, ctx->copy_out})

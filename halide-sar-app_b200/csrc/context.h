@@ -17,6 +17,7 @@ struct sarbp_ctx {
     cudaStream_t stream = nullptr;
     sarbp::DeviceBuffer io;  // device copies of host-API inputs and outputs
     sarbp::DeviceBuffer out_aux;
+    sarbp::DeviceBuffer resize_buf;  // resize weights, bounds and intermediates
     std::map<std::string, sarbp_opts> tuned;  // autotuner results by job-set key
     // host-buffer entry points: copies in, second compute stream, copies out,
     // and the events that pipeline row slabs between them

@@ -54,6 +54,19 @@ cudaError_t launch_chunk_tables(const double4 *pulse, const float *wP, int P, in
 cudaError_t launch_finalize(const DevJob *d_job, long long npix, int num_sms, cudaStream_t st);
 cudaError_t launch_fill_items(WorkItem *items, int ntiles, RowItem *rows, int nrows, cudaStream_t st);
 
+// resize.cu (the reference's data/resize.py resampling)
+struct ResizePlan {
+    int elem_bytes;        // 4 (f32) or 8 (f64)
+    int nc;                // interleaved components resampled independently
+    int rows, cols, orows, ocols;
+    double zoom[2];        // input / output extent per axis
+    int radius[2];         // Gaussian radius per axis; -1: axis not filtered
+    int woff[2];           // offset of each axis's weights w[0..radius] in d_weights
+    const double *d_weights;
+};
+cudaError_t launch_resize(const ResizePlan &p, const void *in, void *out, void *tmp_a, void *tmp_b,
+                          double *bounds, cudaStream_t st);
+
 // peaks.cu
 cudaError_t measure_peaks(int num_sms, cudaStream_t st, double *ffma_per_s, double *mufu_per_s);
 

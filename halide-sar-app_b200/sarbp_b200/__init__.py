@@ -240,6 +240,34 @@ class Context:
         check(lib().sarbp_img_output_u8_from_img_device(self._h, ctypes.c_void_p(img_ptr), int(nu), int(nv),
                                                         float(dB_min), float(dB_max), ctypes.c_void_p(out_ptr)))
 
+    def resize(self, a, shape):
+        """skimage.transform.resize(a, shape, preserve_range=True) as the
+        reference's data/resize.py uses it, on the device (sarbp_resize):
+        a 1-D or 2-D f32 / f64 array; a complex array is resampled as its
+        real and imaginary parts."""
+        a = np.asarray(a)
+        shape = tuple(int(x) for x in shape)
+        if a.ndim not in (1, 2) or len(shape) != a.ndim:
+            raise SarbpError(ERR_INVALID, "resize: 1-D or 2-D arrays, and a shape of the same rank")
+        cplx = np.iscomplexobj(a)
+        if cplx:
+            real = np.float32 if a.dtype == np.complex64 else np.float64
+            src = np.ascontiguousarray(a).view(real)
+        else:
+            if a.dtype not in (np.float32, np.float64):
+                a = a.astype(np.float64)
+            real = a.dtype.type
+            src = np.ascontiguousarray(a)
+        rows, cols = (1, a.shape[0]) if a.ndim == 1 else a.shape
+        orows, ocols = (1, shape[0]) if a.ndim == 1 else shape
+        nc = 2 if cplx else 1
+        out = np.empty((orows, ocols * nc), real)
+        check(lib().sarbp_resize(self._h, np.dtype(real).itemsize, nc, _ptr(src), rows, cols, orows, ocols,
+                                 _ptr(out)))
+        if cplx:
+            out = out.view(np.complex64 if real == np.float32 else np.complex128)
+        return out.reshape(shape)
+
     def range_compress_device(self, job, q_out_ptr, precision=None):
         """Writes the complex64 range profiles [P, N_fft] of `job` to q_out_ptr."""
         o = _opts(precision)
@@ -360,7 +388,7 @@ class Server:
         self._keep[rid.value] = (job, keep)
         return rid.value
 
-    def register(self, job, keep=None):
+    def register(self, job):
         """Uploads and range-compresses an aperture (a Job of host pointers)
         once; returns its id for submit_on."""
         aid = ctypes.c_longlong()

@@ -139,6 +139,10 @@ SIGNATURES = {
                                                   ctypes.c_double, ctypes.c_double, _dp]),
     "sarbp_img_output_u8_from_img_device": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int,
                                                            ctypes.c_double, ctypes.c_double, _dp]),
+    "sarbp_resize_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp]),
+    "sarbp_resize": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp]),
     "sarbp_taylor": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, _dp]),
     "sarbp_taylor_mode": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp]),
     "sarbp_img_plane_dims": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _c_int_p,

@@ -11,9 +11,10 @@ and geometry scale:
   plain_large  1999 x 1024, f0 16.7 GHz, 0.59 MHz step, 8 km, 45 deg,
                3 deg span, 200 scatterers + uniform-amplitude clutter grid,
                2048^2 image over 100 m, Taylor 30, upsample 2, dB -45..0
+  plain_mid    plain_large's aperture on a 1024^2 image over 50 m
   precision    4000 x 2048 at 20 km, 300 scatterers, 4096^2 image
   batch        96 uneven jobs (image 256^2..2048^2, 128-2000 pulses,
-               256/512/1024 samples, Taylor 17-35, 5-15 km, 20-50 deg)
+               256/512/1024 samples, Taylor 17-35 dB, 5-15 km, 20-50 deg)
 
 Each scene is a list of point scatterers (x, y, z, Re a, Im a); the phase
 history is S(f, p) = sum_i a_i exp(+j 4 pi f / c (|p| - |p - x_i|)) plus
@@ -35,6 +36,10 @@ CONFIGS = {
     "plain_large": dict(P=1999, S=1024, f0=16.7e9, df=0.59e6, R0=8e3, dep=45.0, span=3.0,
                         nscat=200, half=45.0, clutter=32, snr=20.0, n=2048, extent=100.0,
                         taylor=30, upsample=2, db=(-45.0, 0.0)),
+    # plain_large's aperture on a 1024^2 image over 50 m (profiling captures)
+    "plain_mid": dict(P=1999, S=1024, f0=16.7e9, df=0.59e6, R0=8e3, dep=45.0, span=3.0,
+                      nscat=200, half=22.0, clutter=32, snr=20.0, n=1024, extent=50.0,
+                      taylor=30, upsample=2, db=(-45.0, 0.0)),
     "precision": dict(P=4000, S=2048, f0=16.7e9, df=0.59e6, R0=20e3, dep=45.0, span=3.0,
                       nscat=300, half=45.0, clutter=32, snr=20.0, n=4096, extent=100.0,
                       taylor=30, upsample=2, db=(-45.0, 0.0)),

@@ -407,6 +407,25 @@ int sarbp_img_output_u8_from_img_device(sarbp_ctx *ctx, const double *img, int n
                                         int nv, double dB_min, double dB_max,
                                         uint8_t *out);
 
+/*
+ * Resampling of platform arrays to other pulse / sample counts: the
+ * computation of the reference's data/resize.py (data/resize.py:14-70),
+ * skimage.transform.resize(a, (out_rows, out_cols), preserve_range=True)
+ * with its defaults -- linear interpolation on grid-aligned sample
+ * positions, mirrored edges, a Gaussian anti-aliasing filter of sigma
+ * (in/out - 1)/2 on the axes that shrink (when any axis shrinks), output
+ * clipped to the input's range -- restated on the device.  `in`/`out` are
+ * [rows][cols][ncomp] arrays of f32 (elem_bytes 4) or f64 (8); the ncomp
+ * interleaved components (re, im of a complex array) are resampled
+ * independently.  A 1-D array is rows = 1.  The _device form takes device
+ * pointers and is enqueued on the context's stream; sarbp_resize takes host
+ * pointers and returns when `out` is written.
+ */
+int sarbp_resize_device(sarbp_ctx *ctx, int elem_bytes, int ncomp, const void *in,
+                        int rows, int cols, int out_rows, int out_cols, void *out);
+int sarbp_resize(sarbp_ctx *ctx, int elem_bytes, int ncomp, const void *in, int rows,
+                 int cols, int out_rows, int out_cols, void *out);
+
 /* ---- host helpers used by the CLI and the harness ---- */
 /* Taylor window (signal.h:14-51), f64 [num]. */
 int sarbp_taylor(int num, double S_L, double *out);
