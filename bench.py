@@ -349,14 +349,22 @@ def run_ours(args, rank, world, local_rank):
     value = world * units * args.steps / (ms_max * 1e-3) / 1e9
 
     # output stage (max|z| + u8 of the complex image), outside the step: the
-    # HBM-bound tail, timed over U8_LAUNCHES back-to-back calls
+    # HBM-bound tail, timed over U8_LAUNCHES back-to-back calls that rotate
+    # over four copies of the image (4 x 67 MB, more than the 126 MB L2)
     t_u8 = torch.empty((nv, nu), dtype=torch.uint8, device=dev)
-    u8_call = lambda: ctx.img_output_u8_from_img_device(t_out.data_ptr(), nu, nv, data["db"][0],
-                                                        data["db"][1], t_u8.data_ptr())
-    for _ in range(3):
+    imgs = [t_out] + [t_out.clone() for _ in range(3)]
+    turn = [0]
+
+    def u8_call():
+        img = imgs[turn[0] % len(imgs)]
+        turn[0] += 1
+        ctx.img_output_u8_from_img_device(img.data_ptr(), nu, nv, data["db"][0], data["db"][1], t_u8.data_ptr())
+
+    for _ in range(4):
         u8_call()
     u8_ms = timed_ms(torch, stream, u8_call, U8_LAUNCHES) / U8_LAUNCHES
     ctx.synchronize()
+    del imgs
 
     # ---- e2e through the host-buffer entry point, pinned host memory ----
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
@@ -448,7 +456,8 @@ def run_ours(args, rank, world, local_rank):
                       "peak": hbm_peak, "unit": "GB/s",
                       "frac": u8_bytes / (u8_ms * 1e-3) / 1e9 / hbm_peak, "bytes": u8_bytes,
                       "how": "sarbp_img_output_u8_from_img_device (max|z| kernel + u8 kernel), "
-                             "%d back-to-back calls" % U8_LAUNCHES},
+                             "%d back-to-back calls over four copies of the image (268 MB > L2)"
+                             % U8_LAUNCHES},
             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s"},
         "e2e": {"value": e2e_value, "unit": "Gpixel*pulses/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms / max(args.e2e_steps, 1),
