@@ -761,7 +761,10 @@ def serve_measure(torch, ctx, dev, rates, nreq, lanes, batch_work, seed, sample_
             rng = np.random.default_rng(int(rate * 1000) + seed)
             pick = rng.integers(0, len(pool), nreq)
             arrive = np.cumsum(rng.exponential(1.0 / rate, nreq))
-            own = set(srng.choice(nreq, max(1, int(round(sample_frac * nreq))), replace=False).tolist())
+            own = srng.choice(nreq, max(1, int(round(sample_frac * nreq))), replace=False).tolist()
+            # the sampled requests' own (pinned) image buffers, made before
+            # the arrivals start: pinning memory is slow and would stall them
+            own = {i: pool[int(pick[i])].new_outputs()[0] for i in own}
             b0 = srv.stats()["batches"]
             rids = []
             start = time.perf_counter()
@@ -772,7 +775,7 @@ def serve_measure(torch, ctx, dev, rates, nreq, lanes, batch_work, seed, sample_
                         break
                     time.sleep(dt if dt > 2e-3 else 0)
                 k = int(pick[i])
-                o = pool[k].new_outputs()[0] if i in own else outs[k]
+                o = own.get(i, outs[k])
                 rids.append((submit(k, o), k, o, i in own))
             lat, first, last, units = [], None, None, 0.0
             for r, k, o, mine in rids:

@@ -60,14 +60,27 @@ __device__ __forceinline__ uint8_t u8_of(double2 z, const U8Scale &u) {
     return to_u8(10.0 * (log(sqrt(a2) / u.m) / kLn10F32), u.lo, u.hi);
 }
 
+// max |z|: four independent 16-byte loads in flight per thread and step (a
+// warp's loads stay contiguous), the maximum taken on |z|^2 and one square
+// root at the end -- the same value, as the square root is monotonic and
+// correctly rounded.
 __global__ void maxabs_kernel(const double2 *__restrict__ img, long long n,
                               unsigned long long *__restrict__ out) {
-    double m = 0.0;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
-        const double2 z = img[i];
-        m = fmax(m, sqrt(z.x * z.x + z.y * z.y));
+    double m2 = 0.0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < n; i += 4 * stride) {
+        double2 z[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) z[k] = img[i + k * stride];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) m2 = fmax(m2, z[k].x * z[k].x + z[k].y * z[k].y);
     }
+    for (; i < n; i += stride) {
+        const double2 z = img[i];
+        m2 = fmax(m2, z.x * z.x + z.y * z.y);
+    }
+    double m = sqrt(m2);
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
     __shared__ double s[32];
     if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = m;
@@ -110,9 +123,12 @@ __global__ void u8_from_db_kernel(const double *__restrict__ dB, long long n, do
 __device__ __forceinline__ void u8_quad(const double2 *__restrict__ img, long long n, long long i0,
                                         uint8_t *__restrict__ u8, bool vec, const U8Scale &us) {
     if (vec && i0 + 4 <= n) {
+        double2 z[4];  // the four loads first, then the conversions
+#pragma unroll
+        for (int k = 0; k < 4; ++k) z[k] = img[i0 + k];
         uint32_t w = 0;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) w |= (uint32_t)u8_of(img[i0 + k], us) << (8 * k);
+        for (int k = 0; k < 4; ++k) w |= (uint32_t)u8_of(z[k], us) << (8 * k);
         *reinterpret_cast<uint32_t *>(u8 + i0) = w;
     } else {
         for (long long i = i0; i < n && i < i0 + 4; ++i) u8[i] = u8_of(img[i], us);
@@ -155,7 +171,10 @@ int grid_for(long long n) {
 }  // namespace
 
 cudaError_t launch_maxabs(const double2 *img, long long n, unsigned long long *d_max, cudaStream_t st) {
-    maxabs_kernel<<<grid_for(n), 256, 0, st>>>(img, n, d_max);
+    // at least eight pixels a thread (two steps of four loads), at most
+    // eight 256-thread blocks per SM
+    const long long b = std::max<long long>(1, std::min<long long>((n + 2047) / 2048, 148LL * 8));
+    maxabs_kernel<<<(unsigned)b, 256, 0, st>>>(img, n, d_max);
     return cudaGetLastError();
 }
 

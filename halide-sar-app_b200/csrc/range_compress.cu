@@ -186,11 +186,8 @@ __device__ __forceinline__ void passes16(float2 (&v)[16], int t, float2 *sm, con
     }
 }
 
-// N_fft 4096 (256 threads a row, 34.8 KB of exchange buffer): registers
-// capped for 5 CTAs per SM instead of the 4 that 64 registers allow, so
-// that the 1999 rows of a 2048^2 x 1999 job run in 3 waves instead of 4.
 template <int LOGN>
-__global__ void __launch_bounds__((1 << LOGN) / 16 > 256 ? (1 << LOGN) / 16 : 256, LOGN == 12 ? 5 : 1)
+__global__ void __launch_bounds__((1 << LOGN) / 16 > 256 ? (1 << LOGN) / 16 : 256)
 range_compress_kernel(const DevJob *__restrict__ jobs, const RowItem *__restrict__ rows, int nrows,
                       const float2 *__restrict__ tw, int pairs) {
     constexpr int N = 1 << LOGN;

@@ -175,8 +175,9 @@ def test_misuse_is_an_error_code(sb, ctx):
         assert e.value.code == _lib.ERR_STATE
     finally:
         acc.close()
+    jobs[1].precision = sb.PREC_NAIVE
     with pytest.raises(sb.SarbpError) as e:
-        sb.Accumulator(ctx, jobs[1], 10, precision=sb.PREC_NAIVE)
+        sb.Accumulator(ctx, jobs[1], 10)
     assert e.value.code == _lib.ERR_UNSUPPORTED
 
 
