@@ -168,12 +168,26 @@ int grid_for(long long n) {
     return (int)b;
 }
 
+// CTAs of 256 threads that the device holds at once for `kernel` (one wave
+// of a grid-stride loop: no partial last wave); looked up once per kernel.
+template <typename K>
+long long resident_ctas(K kernel, int *cache) {
+    if (*cache > 0) return *cache;
+    int dev = 0, sms = 148, occ = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, 256, 0) != cudaSuccess || occ < 1) occ = 4;
+    *cache = occ * sms;
+    return *cache;
+}
+int g_maxabs_ctas = 0, g_img_u8_ctas = 0, g_batch_u8_ctas = 0;
+
 }  // namespace
 
 cudaError_t launch_maxabs(const double2 *img, long long n, unsigned long long *d_max, cudaStream_t st) {
-    // at least eight pixels a thread (two steps of four loads), at most
-    // eight 256-thread blocks per SM
-    const long long b = std::max<long long>(1, std::min<long long>((n + 2047) / 2048, 148LL * 8));
+    // at least eight pixels a thread (two steps of four loads), at most one
+    // wave of resident CTAs
+    const long long b = std::max<long long>(
+        1, std::min<long long>((n + 2047) / 2048, resident_ctas(maxabs_kernel, &g_maxabs_ctas)));
     maxabs_kernel<<<(unsigned)b, 256, 0, st>>>(img, n, d_max);
     return cudaGetLastError();
 }
@@ -192,16 +206,18 @@ cudaError_t launch_u8_from_db(const double *dB, long long n, double lo, double h
 
 cudaError_t launch_img_u8(const double2 *img, long long n, const unsigned long long *d_max, uint8_t *u8,
                           double lo, double hi, cudaStream_t st) {
-    // about eight 256-thread blocks per SM, four pixels per thread
-    const long long bx = std::max<long long>(1, std::min<long long>((n / 4 + 255) / 256, 148LL * 8));
+    // one wave of resident CTAs, four pixels per thread and step
+    const long long bx = std::max<long long>(
+        1, std::min<long long>((n / 4 + 255) / 256, resident_ctas(img_u8_kernel, &g_img_u8_ctas)));
     img_u8_kernel<<<(unsigned)bx, 256, 0, st>>>(img, n, d_max, u8, lo, hi);
     return cudaGetLastError();
 }
 
 cudaError_t launch_batch_u8(const DevJob *d_jobs, int njobs, long long max_pixels, cudaStream_t st) {
-    // about eight 256-thread blocks per SM over the whole batch
+    // one wave of resident CTAs over the whole batch
     long long bx = (max_pixels / 4 + 255) / 256;
-    const long long cap = std::max<long long>(1, (148LL * 8 + njobs - 1) / njobs);
+    const long long cap =
+        std::max<long long>(1, (resident_ctas(batch_u8_kernel, &g_batch_u8_ctas) + njobs - 1) / njobs);
     bx = std::max<long long>(1, std::min(bx, cap));
     batch_u8_kernel<<<dim3((unsigned)bx, njobs), 256, 0, st>>>(d_jobs);
     return cudaGetLastError();
