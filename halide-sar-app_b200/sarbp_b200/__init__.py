@@ -25,8 +25,9 @@ from ._lib import (ERR_ADMISSION, ERR_CUDA, ERR_GEOMETRY, ERR_INVALID, ERR_NOMEM
 
 __all__ = [
     "Context", "Job", "Opts", "SarbpError", "PREC_COMPAT", "PREC_PRECISE", "PREC_NAIVE",
-    "TAYLOR_REF", "TAYLOR_FLOAT",
-    "n_fft_for", "taylor", "img_plane_create", "img_plane_dims", "pixel_locs", "version",
+    "TAYLOR_REF", "TAYLOR_FLOAT", "Accumulator", "Server", "Plan", "make_job", "job_device_bytes",
+    "backprojection_streamed", "n_fft_for", "taylor", "img_plane_create", "img_plane_dims", "pixel_locs",
+    "version",
 ]
 
 

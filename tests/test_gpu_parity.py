@@ -369,6 +369,24 @@ def test_db_u8_kernels_match_oracle(ctx, oracle, cfg1):
     np.testing.assert_array_equal(u8, oracle.img_output_u8(dBr, -30.0, 0.0))
 
 
+@pytest.mark.parametrize("shape", [(300, 257), (512, 512), (1, 3)])
+def test_u8_from_image_in_one_pass_matches_oracle(ctx, oracle, torch, shape):
+    """sarbp_img_output_u8_from_img_device (max|z| then grey levels, no f64
+    dB image) gives exactly the reference's u8 of the image
+    (img_output.cpp:18-51 through the oracle), also for ragged sizes."""
+    rng = np.random.default_rng(11)
+    img = (rng.normal(size=shape) + 1j * rng.normal(size=shape)) * rng.uniform(0, 5, shape)
+    nv, nu = shape
+    for lo, hi in ((-30.0, 0.0), (-3.0, -1.0)):
+        d_img = torch.from_numpy(img.view(np.float64).reshape(nv, nu, 2).copy()).cuda()
+        d_u8 = torch.zeros((nv, nu), dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        ctx.img_output_u8_from_img_device(d_img.data_ptr(), nu, nv, lo, hi, d_u8.data_ptr())
+        ctx.synchronize()
+        want = oracle.img_output_u8(oracle.img_output_to_dB(img), lo, hi)
+        assert np.array_equal(d_u8.cpu().numpy(), want), (shape, lo, hi)
+
+
 def test_naive_mode_is_worse_but_finite(ctx, oracle, cfg1):
     d = cfg1
     ref = oracle.backprojection(d["phs"], d["k_r"], d["taylor"], d["N_fft"], d["delta_r"], d["pos"],
