@@ -82,8 +82,9 @@ BpLaunch launch_for(const sarbp_opts *opts, int num_sms) {
     return L;
 }
 
-// Device bytes of a job's own inputs and outputs (host-buffer paths).
-size_t io_bytes(const sarbp_job &j, bool with_phs) {
+}  // namespace
+
+size_t sarbp::job_io_bytes(const sarbp_job &j, bool with_phs) {
     const size_t P = (size_t)j.npulses, S = (size_t)j.nsamples, npix = (size_t)j.nu * j.nv;
     size_t b = with_phs ? a256(P * S * 8) : 0;
     b += j.k_r ? a256(S * 4) : 0;
@@ -96,6 +97,8 @@ size_t io_bytes(const sarbp_job &j, bool with_phs) {
     return b;
 }
 
+namespace {
+size_t io_bytes(const sarbp_job &j, bool with_phs) { return job_io_bytes(j, with_phs); }
 }  // namespace
 
 struct sarbp_accum {
@@ -117,9 +120,13 @@ struct sarbp_accum {
     cudaEvent_t copied[2] = {nullptr, nullptr}, consumed[2] = {nullptr, nullptr};
     bool finalized = false;
 
+    // streams of the serving loop's streaming apertures (NULL: the context's)
+    cudaStream_t own_st = nullptr, own_cin = nullptr;
+
     char *dptr(size_t off) const { return static_cast<char *>(mem.ptr) + off; }
     DevJob *d_job() const { return reinterpret_cast<DevJob *>(dptr(lay.job)); }
-    cudaStream_t st() const { return ctx->stream; }
+    cudaStream_t st() const { return own_st ? own_st : ctx->stream; }
+    cudaStream_t cin() const { return own_cin ? own_cin : ctx->copy_in; }
     int start();
     int check_chunk(int q0, int n) const;
     int add(int q0, int n, const float *phs_rows, cudaEvent_t rc_done);
@@ -208,10 +215,8 @@ int sarbp_accum::add(int q0, int n, const float *phs_rows, cudaEvent_t rc_done) 
     return SARBP_OK;
 }
 
-extern "C" {
-
-int sarbp_accum_create(sarbp_ctx *ctx, const sarbp_job *job, const sarbp_opts *opts, int max_chunk,
-                       sarbp_accum **out) {
+int sarbp::accum_create_on(sarbp_ctx *ctx, const sarbp_job *job, const sarbp_opts *opts, int max_chunk,
+                           cudaStream_t stream, cudaStream_t copy_stream, sarbp_accum **out) {
     int rc = ctx_set_device(ctx);
     if (rc) return rc;
     if (!job || !out) return fail(SARBP_ERR_INVALID, "job and out must be non-NULL");
@@ -224,6 +229,8 @@ int sarbp_accum_create(sarbp_ctx *ctx, const sarbp_job *job, const sarbp_opts *o
     if (max_chunk < 1) return fail(SARBP_ERR_INVALID, "max_chunk must be >= 1");
     std::unique_ptr<sarbp_accum> a(new sarbp_accum());
     a->ctx = ctx;
+    a->own_st = stream;
+    a->own_cin = copy_stream;
     a->job = *job;
     a->prec = prec;
     a->L = launch_for(opts, ctx->dev.num_sms);
@@ -263,6 +270,13 @@ int sarbp_accum_create(sarbp_ctx *ctx, const sarbp_job *job, const sarbp_opts *o
     return SARBP_OK;
 }
 
+extern "C" {
+
+int sarbp_accum_create(sarbp_ctx *ctx, const sarbp_job *job, const sarbp_opts *opts, int max_chunk,
+                       sarbp_accum **out) {
+    return accum_create_on(ctx, job, opts, max_chunk, nullptr, nullptr, out);
+}
+
 int sarbp_accum_add_device(sarbp_accum *acc, int pulse0, int count, const float *phs_rows) {
     if (!acc) return fail(SARBP_ERR_INVALID, "accumulator is NULL");
     int rc = ctx_set_device(acc->ctx);
@@ -282,7 +296,7 @@ int sarbp_accum_add(sarbp_accum *acc, int pulse0, int count, const float *phs_ro
     if (e != cudaSuccess) return cuda_fail(e, "pulse-chunked job: staging buffers");
     const int b = (int)(acc->nhost & 1);
     char *dst = static_cast<char *>(acc->stage.ptr) + b * half;
-    cudaStream_t cin = acc->ctx->copy_in;
+    cudaStream_t cin = acc->cin();
     // the chunk that used this staging buffer two adds ago must be range-compressed
     if (acc->nhost >= 2 && (e = cudaStreamWaitEvent(cin, acc->consumed[b], 0)) != cudaSuccess)
         return cuda_fail(e, "cudaStreamWaitEvent");
@@ -334,7 +348,7 @@ int sarbp_accum_wait(sarbp_accum *acc) {
     int rc = ctx_set_device(acc->ctx);
     if (rc) return rc;
     cudaError_t e = cudaStreamSynchronize(acc->st());
-    if (e == cudaSuccess) e = cudaStreamSynchronize(acc->ctx->copy_in);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(acc->cin());
     if (e != cudaSuccess) return cuda_fail(e, "synchronising the stream");
     if (!acc->finalized) return SARBP_OK;
     const int s = static_cast<const JobScalars *>(acc->status_pin.ptr)->status;
@@ -371,7 +385,7 @@ int sarbp_accum_destroy(sarbp_accum *acc) {
     if (!acc) return SARBP_OK;
     cudaSetDevice(acc->ctx->dev.device);
     cudaStreamSynchronize(acc->st());
-    cudaStreamSynchronize(acc->ctx->copy_in);
+    cudaStreamSynchronize(acc->cin());
     acc->mem.release();
     acc->stage.release();
     acc->status_pin.release();
@@ -388,14 +402,15 @@ int sarbp_job_device_bytes(const sarbp_job *job, const sarbp_opts *opts, int chu
     if (job->npulses < 1 || job->nsamples < 1 || job->nu < 1 || job->nv < 1 || job->n_fft < 1)
         return fail(SARBP_ERR_INVALID, "sizes must be >= 1");
     const BpLaunch L = launch_for(opts, 148);
-    if (chunk_pulses <= 0 || chunk_pulses >= job->npulses) {
+    if (chunk_pulses <= 0) {
         sarbp_job j = *job;
         j.precision = precision_for(*job, opts);
         *bytes = (double)(io_bytes(*job, true) + Runner::job_scratch_bytes(j, opts));
         return SARBP_OK;
     }
-    const size_t stage = 2 * a256((size_t)chunk_pulses * job->nsamples * 8);
-    *bytes = (double)(io_bytes(*job, false) + accum_layout(*job, L.tile_x, L.tile_y, chunk_pulses).end + stage);
+    const int C = std::min(chunk_pulses, job->npulses);
+    const size_t stage = 2 * a256((size_t)C * job->nsamples * 8);
+    *bytes = (double)(io_bytes(*job, false) + accum_layout(*job, L.tile_x, L.tile_y, C).end + stage);
     return SARBP_OK;
 }
 

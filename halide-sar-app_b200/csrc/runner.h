@@ -152,3 +152,16 @@ int validate_job(const sarbp_job &j, int prec, int idx, bool rc_only, bool need_
 void describe_job(const sarbp_job &j, int prec, int tile_x, int tile_y, DevJob &dj);
 
 }  // namespace sarbp
+
+struct sarbp_ctx;
+struct sarbp_accum;
+namespace sarbp {
+// sarbp_accum_create on the given compute and copy streams instead of the
+// context's (the serving loop's streaming apertures); NULL: the context's.
+int accum_create_on(sarbp_ctx *ctx, const sarbp_job *job, const sarbp_opts *opts, int max_chunk,
+                    cudaStream_t stream, cudaStream_t copy_stream, sarbp_accum **out);
+// Device bytes of a job's inputs other than its phase history, and its
+// outputs (the host-buffer paths' device copies).
+size_t job_io_bytes(const sarbp_job &j, bool with_phs);
+
+}  // namespace sarbp

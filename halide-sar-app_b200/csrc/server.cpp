@@ -70,6 +70,27 @@ struct Aperture {
     int refs = 0;  // queued or running requests on it
 };
 
+// A streaming aperture: a device-resident partial image (pulse-chunked
+// accumulator) with its own compute and copy streams, and the device copies
+// of the job's inputs other than the phase history, and of its outputs.
+struct StreamAp {
+    sarbp_job host{};      // the caller's job (host outputs)
+    sarbp_job dev{};       // device copies
+    DeviceBuffer io;
+    sarbp_accum *acc = nullptr;
+    size_t bytes = 0;      // charged to the budget
+    cudaStream_t st = nullptr, cin = nullptr;
+    void release() {
+        if (acc) sarbp_accum_destroy(acc);
+        acc = nullptr;
+        if (st) cudaStreamSynchronize(st);
+        io.release();
+        if (st) cudaStreamDestroy(st);
+        if (cin) cudaStreamDestroy(cin);
+        st = cin = nullptr;
+    }
+};
+
 struct Request {
     long long id = 0;
     Aperture *ap = nullptr;  // registered aperture, or NULL (the request brings its phase history)
@@ -139,6 +160,9 @@ struct sarbp_server {
     std::thread sched, comp;
     // registered apertures (guarded by mu) and their set-up stream
     std::map<long long, std::unique_ptr<Aperture>> apertures;
+    // streaming apertures: partial images accumulating pulse chunks
+    std::map<long long, std::unique_ptr<StreamAp>> streams;
+    long long next_stream = 1;
     long long next_ap = 1;
     cudaStream_t reg_st = nullptr;
     // counters: bytes copied host -> device, pulses range-compressed,
@@ -502,6 +526,8 @@ int sarbp_server_destroy(sarbp_server *s) {
         if (L.st) cudaStreamDestroy(L.st);
         if (L.done) cudaEventDestroy(L.done);
     }
+    for (auto &kv : s->streams) kv.second->release();
+    s->streams.clear();
     for (auto &kv : s->apertures) cudaFreeAsync(kv.second->mem, s->reg_st);
     s->apertures.clear();
     if (s->reg_st) {
@@ -702,6 +728,131 @@ int sarbp_server_unregister(sarbp_server *s, long long aperture) {
     s->cv.notify_all();
     if (e != cudaSuccess) return cuda_fail(e, "unregistering an aperture");
     return SARBP_OK;
+}
+
+int sarbp_server_open_stream(sarbp_server *s, const sarbp_job *host_job, int max_chunk, long long *stream_id) {
+    if (!s || !host_job || !stream_id) return fail(SARBP_ERR_INVALID, "bad open_stream arguments");
+    int rc = ctx_set_device(s->ctx);
+    if (rc) return rc;
+    sarbp_job h = *host_job;
+    if (h.precision < 0) h.precision = s->launch.precision;
+    if (h.precision != SARBP_PREC_COMPAT && h.precision != SARBP_PREC_PRECISE)
+        return fail(SARBP_ERR_UNSUPPORTED, "streaming apertures run SARBP_PREC_COMPAT or SARBP_PREC_PRECISE");
+    rc = validate_job(h, h.precision, 0, false, false);
+    if (rc) return rc;
+    if (max_chunk < 1) return fail(SARBP_ERR_INVALID, "max_chunk must be >= 1");
+    double need = 0;
+    rc = sarbp_job_device_bytes(&h, &s->launch, max_chunk, &need);
+    if (rc) return rc;
+    auto sa = std::make_unique<StreamAp>();
+    sa->bytes = (size_t)need;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->in_use + sa->bytes > s->cap)
+            return fail(SARBP_ERR_ADMISSION, "streaming aperture needs " + std::to_string(sa->bytes >> 20) +
+                                                 " MiB of device memory; the budget has " +
+                                                 std::to_string((s->cap - std::min(s->cap, s->in_use)) >> 20) +
+                                                 " MiB free");
+        s->in_use += sa->bytes;
+        s->peak = std::max(s->peak, s->in_use);
+    }
+    auto undo = [&](int code) {
+        sa->release();
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->in_use -= sa->bytes;
+        s->cv.notify_all();
+        return code;
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&sa->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sa->cin, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = sa->io.alloc_exact(job_io_bytes(h, false));
+    if (e != cudaSuccess) return undo(cuda_fail(e, "streaming aperture: streams and device memory"));
+    // inputs other than the phase history, and the outputs, on the device
+    const size_t P = (size_t)h.npulses, S = (size_t)h.nsamples, npix = (size_t)h.nu * h.nv;
+    char *b = static_cast<char *>(sa->io.ptr);
+    size_t o = 0;
+    sarbp_job d = h;
+    auto put = [&](const void *src, size_t n) -> const void * {
+        if (!src) return nullptr;
+        void *p = b + o;
+        o += (n + 255) / 256 * 256;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(p, src, n, cudaMemcpyHostToDevice, sa->st);
+        return p;
+    };
+    d.k_r = static_cast<const float *>(put(h.k_r, S * 4));
+    d.k_r64 = static_cast<const double *>(put(h.k_r64, S * 8));
+    d.pos = static_cast<const float *>(put(h.pos, P * 12));
+    d.pos64 = static_cast<const double *>(put(h.pos64, P * 24));
+    d.r = static_cast<const double *>(put(h.r, npix * 24));
+    d.u = h.r ? nullptr : static_cast<const double *>(put(h.u, (size_t)h.nu * 8));
+    d.v = h.r ? nullptr : static_cast<const double *>(put(h.v, (size_t)h.nv * 8));
+    d.phs = nullptr;
+    d.output_img = reinterpret_cast<double *>(b + o);
+    o += (npix * 16 + 255) / 256 * 256;
+    d.out_u8 = h.out_u8 ? reinterpret_cast<uint8_t *>(b + o) : nullptr;
+    if (e != cudaSuccess) return undo(cuda_fail(e, "streaming aperture: copying inputs"));
+    s->h2d_bytes += (long long)o;
+    rc = accum_create_on(s->ctx, &d, &s->launch, max_chunk, sa->st, sa->cin, &sa->acc);
+    if (rc) {
+        const std::string msg = last_error_cstr();
+        undo(rc);
+        return fail(rc, msg);
+    }
+    sa->host = h;
+    sa->dev = d;
+    std::lock_guard<std::mutex> lk(s->mu);
+    *stream_id = s->next_stream++;
+    s->streams[*stream_id] = std::move(sa);
+    return SARBP_OK;
+}
+
+int sarbp_server_stream_add(sarbp_server *s, long long stream_id, int pulse0, int count,
+                            const float *phs_rows_host) {
+    if (!s) return fail(SARBP_ERR_INVALID, "server is NULL");
+    StreamAp *sa = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->streams.find(stream_id);
+        if (it == s->streams.end()) return fail(SARBP_ERR_INVALID, "unknown stream id");
+        sa = it->second.get();
+    }
+    const int rc = sarbp_accum_add(sa->acc, pulse0, count, phs_rows_host);
+    if (rc == SARBP_OK) {
+        s->h2d_bytes += (long long)count * sa->host.nsamples * 8;
+        s->rc_pulses += count;
+    }
+    return rc;
+}
+
+int sarbp_server_stream_finish(sarbp_server *s, long long stream_id) {
+    if (!s) return fail(SARBP_ERR_INVALID, "server is NULL");
+    std::unique_ptr<StreamAp> sa;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->streams.find(stream_id);
+        if (it == s->streams.end()) return fail(SARBP_ERR_INVALID, "unknown stream id");
+        sa = std::move(it->second);
+        s->streams.erase(it);
+    }
+    int rc = ctx_set_device(s->ctx);
+    if (rc == SARBP_OK) rc = sarbp_accum_finalize(sa->acc);
+    if (rc == SARBP_OK) {
+        const size_t npix = (size_t)sa->host.nu * sa->host.nv;
+        cudaError_t e = cudaSuccess;
+        if (sa->host.output_img)
+            e = cudaMemcpyAsync(sa->host.output_img, sa->dev.output_img, npix * 16, cudaMemcpyDeviceToHost, sa->st);
+        if (e == cudaSuccess && sa->host.out_u8)
+            e = cudaMemcpyAsync(sa->host.out_u8, sa->dev.out_u8, npix, cudaMemcpyDeviceToHost, sa->st);
+        rc = e == cudaSuccess ? sarbp_accum_wait(sa->acc) : cuda_fail(e, "streaming aperture: copying the image");
+    }
+    const std::string msg = rc ? last_error_cstr() : std::string();
+    sa->release();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->in_use -= sa->bytes;
+        s->cv.notify_all();
+    }
+    return rc ? fail(rc, msg) : SARBP_OK;
 }
 
 int sarbp_server_counters(sarbp_server *s, double *h2d_bytes, long long *rc_pulses,

@@ -407,6 +407,28 @@ class Server:
     def unregister(self, aperture):
         check(lib().sarbp_server_unregister(self._h, int(aperture)))
 
+    def open_stream(self, job, max_chunk):
+        """A streaming aperture (partial image on the device) for a Job of host
+        pointers whose phase history will arrive in chunks; returns its id."""
+        sid = ctypes.c_longlong()
+        check(lib().sarbp_server_open_stream(self._h, ctypes.byref(job), int(max_chunk), ctypes.byref(sid)))
+        self._keep[("stream", sid.value)] = [job]
+        return sid.value
+
+    def stream_add(self, stream, pulse0, rows):
+        """Adds host phase-history rows (complex64 [count, S]) starting at pulse0."""
+        rows = np.ascontiguousarray(rows, np.complex64)
+        check(lib().sarbp_server_stream_add(self._h, int(stream), int(pulse0), int(rows.shape[0]), _ptr(rows)))
+        # these rows may still be read by their copy until the next add returns
+        self._keep[("stream", stream)][1:] = [rows]
+
+    def stream_finish(self, stream):
+        """Writes the stream's image into its output buffer(s) and frees it."""
+        try:
+            check(lib().sarbp_server_stream_finish(self._h, int(stream)))
+        finally:
+            self._keep.pop(("stream", stream), None)
+
     def counters(self):
         """(bytes copied host -> device, pulses range-compressed, requests
         served from registered apertures) since the server started."""

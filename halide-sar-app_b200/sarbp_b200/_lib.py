@@ -105,6 +105,11 @@ SIGNATURES = {
     "sarbp_server_submit_on": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(Job),
                                               ctypes.POINTER(ctypes.c_longlong)]),
     "sarbp_server_unregister": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
+    "sarbp_server_open_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job), ctypes.c_int,
+                                                ctypes.POINTER(ctypes.c_longlong)]),
+    "sarbp_server_stream_add": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                               _dp]),
+    "sarbp_server_stream_finish": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     "sarbp_server_counters": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     "sarbp_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job), ctypes.c_int,

@@ -260,6 +260,29 @@ int sarbp_server_register(sarbp_server *server, const sarbp_job *host_aperture,
 int sarbp_server_submit_on(sarbp_server *server, long long aperture,
                            const sarbp_job *host_job, long long *id);
 int sarbp_server_unregister(sarbp_server *server, long long aperture);
+/*
+ * Streaming apertures: a partial image kept on the device while an
+ * aperture's phase history arrives in pulse chunks (a pulse-chunked
+ * accumulator, sarbp_accum_*, under the server's budget and beside its
+ * batches).  sarbp_server_open_stream takes a job of HOST pointers (k_r,
+ * antenna positions of all npulses pulses, image plane, output_img and
+ * optional out_u8; phs is not read), charges its device footprint
+ * (sarbp_job_device_bytes with max_chunk) to the budget
+ * (SARBP_ERR_ADMISSION when it does not fit) and uploads those inputs;
+ * sarbp_server_stream_add range-compresses host phase-history rows
+ * [pulse0, pulse0 + count) and adds them to the partial image on the
+ * stream's own streams, overlapped with the lanes' batches (the rows may be
+ * reused once the next add or the finish returns); sarbp_server_stream_finish
+ * applies the final phase and row flip, copies the image(s) to the host,
+ * waits, frees the stream and returns its status.  Calls for one stream
+ * come from one host thread at a time.
+ */
+int sarbp_server_open_stream(sarbp_server *server, const sarbp_job *host_job,
+                             int max_chunk, long long *stream_id);
+int sarbp_server_stream_add(sarbp_server *server, long long stream_id, int pulse0,
+                            int count, const float *phs_rows_host);
+int sarbp_server_stream_finish(sarbp_server *server, long long stream_id);
+
 /* Bytes the server copied host -> device, pulses it range-compressed, and
  * requests it served from registered apertures, since it started. */
 int sarbp_server_counters(sarbp_server *server, double *h2d_bytes,
@@ -320,9 +343,9 @@ int sarbp_accum_destroy(sarbp_accum *acc);
 
 /*
  * Device bytes a job needs: its inputs and outputs plus the library's
- * scratch, formed in one call (chunk_pulses <= 0 or >= npulses) or in
- * pulse chunks of chunk_pulses with two staging buffers (the phase history
- * itself then never resides whole).
+ * scratch, formed in one call (chunk_pulses <= 0) or through a pulse-chunked
+ * accumulator with chunks of min(chunk_pulses, npulses) pulses and two
+ * staging buffers (the phase history itself then never resides whole).
  */
 int sarbp_job_device_bytes(const sarbp_job *job, const sarbp_opts *opts,
                            int chunk_pulses, double *bytes);

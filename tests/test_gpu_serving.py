@@ -173,3 +173,65 @@ def test_register_over_budget_is_an_admission_error(ctx, sb):
         assert srv.stats()["in_use_bytes"] == 0
     finally:
         srv.close()
+
+
+def test_streaming_aperture_beside_batches(ctx, sb, pool):
+    """A streaming aperture (partial image on the device, phase history
+    arriving in chunks) under the server's budget, while requests run: its
+    image equals the stand-alone pulse-chunked accumulator's bit for bit and
+    the one-shot image to 1e-5; its device memory is charged while open and
+    returned at finish; one that does not fit is an admission error."""
+    import torch
+    from sarbp_b200 import _lib
+    hj = pool[2]
+    d = hj.data
+    srv = sb.Server(ctx, hbm_cap_bytes=8e9, lanes=2, max_batch=8, precision=sb.PREC_PRECISE)
+    try:
+        base = srv.stats()["in_use_bytes"]
+        out_s = hj.new_outputs()[0]
+        sid = srv.open_stream(hj.job(out_s, precision=sb.PREC_PRECISE), 64)
+        assert srv.stats()["in_use_bytes"] > base
+        rids = [_submit(srv, pool[i % len(pool)], sb.PREC_PRECISE)[0] for i in range(6)]
+        chunks = [(q, min(64, hj.P - q)) for q in range(0, hj.P, 64)]
+        for q0, n in chunks:
+            srv.stream_add(sid, q0, d["phs"][q0:q0 + n])
+        srv.stream_finish(sid)
+        for r in rids:
+            assert srv.wait(r, 60.0) == 0
+        assert srv.stats()["in_use_bytes"] == base
+        with pytest.raises(sb.SarbpError) as e:
+            srv.stream_add(sid, 0, d["phs"][:1])
+        assert e.value.code == _lib.ERR_INVALID
+    finally:
+        srv.close()
+    # the stand-alone accumulator and the one-shot image on the same data
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    t = dict(phs=dev(d["phs"].view(np.float32)), k=dev(d["k_r"].astype(np.float32)), k64=dev(d["k_r"]),
+             pos=dev(d["pos"].astype(np.float32)), pos64=dev(d["pos"]), u=dev(d["u"]), v=dev(d["v"]))
+    outs = [torch.zeros((hj.nv, hj.nu, 2), dtype=torch.float64, device="cuda") for _ in range(2)]
+    jobs = [sb.make_job(hj.S, hj.P, d["N_fft"], d["taylor"], hj.nu, hj.nv, d["delta_r"], t["phs"].data_ptr(),
+                        t["k"].data_ptr(), t["pos"].data_ptr(), o.data_ptr(), u=t["u"].data_ptr(),
+                        v=t["v"].data_ptr(), u_hat=d["u_hat"], v_hat=d["v_hat"], k_r64=t["k64"].data_ptr(),
+                        pos64=t["pos64"].data_ptr(), precision=sb.PREC_PRECISE, taylor_mode=d["taylor_mode"])
+            for o in outs]
+    acc = sb.Accumulator(ctx, jobs[0], 64)
+    try:
+        for q0, n in chunks:
+            acc.add_device(q0, n, t["phs"].data_ptr() + q0 * hj.S * 8)
+        acc.finalize()
+        acc.wait()
+    finally:
+        acc.close()
+    ctx.run_jobs([jobs[1]])
+    ctx.synchronize()
+    alone = outs[0].cpu().numpy().view(np.complex128)[..., 0]
+    one = outs[1].cpu().numpy().view(np.complex128)[..., 0]
+    assert np.array_equal(out_s, alone)
+    assert rel_l2(out_s, one) < 1e-5
+    small = sb.Server(ctx, hbm_cap_bytes=1e6, lanes=1, max_batch=1, precision=sb.PREC_PRECISE)
+    try:
+        with pytest.raises(sb.SarbpError) as e:
+            small.open_stream(hj.job(hj.new_outputs()[0], precision=sb.PREC_PRECISE), 64)
+        assert e.value.code == _lib.ERR_ADMISSION
+    finally:
+        small.close()
