@@ -121,9 +121,11 @@ __device__ __forceinline__ double warp_max_d(double v) {
 }
 
 // GP: pixels per thread (tile pixels / 256: 2, 4 or 8), kept in registers
-// between the two passes; up to 4 the registers fit three CTAs per SM.
+// between the two passes.  Up to 4, registers are sized for four CTAs per
+// SM (64, with a few spills): the kernel is latency-bound, and the extra CTA
+// measured 0.150 ms against 0.157 ms at three (2048^2 x 1999, same output).
 template <int GP>
-__global__ void __launch_bounds__(kThreadsGeom, GP <= 4 ? 3 : 2)
+__global__ void __launch_bounds__(kThreadsGeom, GP <= 4 ? 4 : 2)
     tile_setup_kernel(const DevJob *__restrict__ jobs, const WorkItem *__restrict__ items, int records) {
     constexpr int kWarps = kThreadsGeom / 32;
     __shared__ double sbox[kWarps][6];
