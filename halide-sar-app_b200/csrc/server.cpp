@@ -73,7 +73,11 @@ struct Aperture {
 // A streaming aperture: a device-resident partial image (pulse-chunked
 // accumulator) with its own compute and copy streams, and the device copies
 // of the job's inputs other than the phase history, and of its outputs.
+// Calls on one stream hold `mu`; `closed` is set by the finish, so an add
+// that raced with it (and still held the pointer) sees a closed stream.
 struct StreamAp {
+    std::mutex mu;
+    bool closed = false;
     sarbp_job host{};      // the caller's job (host outputs)
     sarbp_job dev{};       // device copies
     DeviceBuffer io;
@@ -161,7 +165,7 @@ struct sarbp_server {
     // registered apertures (guarded by mu) and their set-up stream
     std::map<long long, std::unique_ptr<Aperture>> apertures;
     // streaming apertures: partial images accumulating pulse chunks
-    std::map<long long, std::unique_ptr<StreamAp>> streams;
+    std::map<long long, std::shared_ptr<StreamAp>> streams;
     long long next_stream = 1;
     long long next_ap = 1;
     cudaStream_t reg_st = nullptr;
@@ -744,7 +748,7 @@ int sarbp_server_open_stream(sarbp_server *s, const sarbp_job *host_job, int max
     double need = 0;
     rc = sarbp_job_device_bytes(&h, &s->launch, max_chunk, &need);
     if (rc) return rc;
-    auto sa = std::make_unique<StreamAp>();
+    auto sa = std::make_shared<StreamAp>();
     sa->bytes = (size_t)need;
     {
         std::lock_guard<std::mutex> lk(s->mu);
@@ -809,13 +813,15 @@ int sarbp_server_open_stream(sarbp_server *s, const sarbp_job *host_job, int max
 int sarbp_server_stream_add(sarbp_server *s, long long stream_id, int pulse0, int count,
                             const float *phs_rows_host) {
     if (!s) return fail(SARBP_ERR_INVALID, "server is NULL");
-    StreamAp *sa = nullptr;
+    std::shared_ptr<StreamAp> sa;
     {
         std::lock_guard<std::mutex> lk(s->mu);
         auto it = s->streams.find(stream_id);
         if (it == s->streams.end()) return fail(SARBP_ERR_INVALID, "unknown stream id");
-        sa = it->second.get();
+        sa = it->second;
     }
+    std::lock_guard<std::mutex> slk(sa->mu);
+    if (sa->closed) return fail(SARBP_ERR_INVALID, "unknown stream id (finished)");
     const int rc = sarbp_accum_add(sa->acc, pulse0, count, phs_rows_host);
     if (rc == SARBP_OK) {
         s->h2d_bytes += (long long)count * sa->host.nsamples * 8;
@@ -826,7 +832,7 @@ int sarbp_server_stream_add(sarbp_server *s, long long stream_id, int pulse0, in
 
 int sarbp_server_stream_finish(sarbp_server *s, long long stream_id) {
     if (!s) return fail(SARBP_ERR_INVALID, "server is NULL");
-    std::unique_ptr<StreamAp> sa;
+    std::shared_ptr<StreamAp> sa;
     {
         std::lock_guard<std::mutex> lk(s->mu);
         auto it = s->streams.find(stream_id);
@@ -834,6 +840,8 @@ int sarbp_server_stream_finish(sarbp_server *s, long long stream_id) {
         sa = std::move(it->second);
         s->streams.erase(it);
     }
+    std::lock_guard<std::mutex> slk(sa->mu);  // after any add in flight
+    sa->closed = true;
     int rc = ctx_set_device(s->ctx);
     if (rc == SARBP_OK) rc = sarbp_accum_finalize(sa->acc);
     if (rc == SARBP_OK) {

@@ -14,6 +14,7 @@ Arrays use the reference's memory layouts (see include/sarbp_b200.h); the
 image comes back as complex128 [nv, nu] with the reference's row flip.
 All compute runs through libsarbp_b200.so; there is no CPU path.
 """
+import collections
 import ctypes
 import math
 
@@ -412,15 +413,17 @@ class Server:
         pointers whose phase history will arrive in chunks; returns its id."""
         sid = ctypes.c_longlong()
         check(lib().sarbp_server_open_stream(self._h, ctypes.byref(job), int(max_chunk), ctypes.byref(sid)))
-        self._keep[("stream", sid.value)] = [job]
+        self._keep[("stream", sid.value)] = [job, collections.deque(maxlen=8)]
         return sid.value
 
     def stream_add(self, stream, pulse0, rows):
         """Adds host phase-history rows (complex64 [count, S]) starting at pulse0."""
         rows = np.ascontiguousarray(rows, np.complex64)
         check(lib().sarbp_server_stream_add(self._h, int(stream), int(pulse0), int(rows.shape[0]), _ptr(rows)))
-        # these rows may still be read by their copy until the next add returns
-        self._keep[("stream", stream)][1:] = [rows]
+        # these rows may still be read by their copy until the next add on the
+        # stream returns; adds from several threads append in any order, so
+        # the last few are kept
+        self._keep[("stream", stream)][1].append(rows)
 
     def stream_finish(self, stream):
         """Writes the stream's image into its output buffer(s) and frees it."""

@@ -274,8 +274,9 @@ int sarbp_server_unregister(sarbp_server *server, long long aperture);
  * stream's own streams, overlapped with the lanes' batches (the rows may be
  * reused once the next add or the finish returns); sarbp_server_stream_finish
  * applies the final phase and row flip, copies the image(s) to the host,
- * waits, frees the stream and returns its status.  Calls for one stream
- * come from one host thread at a time.
+ * waits, frees the stream and returns its status.  Calls on one stream
+ * from several host threads are serialised (an add after the finish
+ * returns SARBP_ERR_INVALID); different streams proceed independently.
  */
 int sarbp_server_open_stream(sarbp_server *server, const sarbp_job *host_job,
                              int max_chunk, long long *stream_id);

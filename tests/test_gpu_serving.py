@@ -235,3 +235,75 @@ def test_streaming_aperture_beside_batches(ctx, sb, pool):
         assert e.value.code == _lib.ERR_ADMISSION
     finally:
         small.close()
+
+
+@pytest.mark.gpu
+def test_streaming_aperture_from_two_threads(ctx, sb, pool):
+    """Two host threads add interleaved pulse chunks to one streaming
+    aperture at once (the library serialises calls on a stream): the image
+    equals the one-thread image to 1e-6 (the chunks' partial sums are added
+    in another order); an add racing the finish either lands before it or is
+    refused as a finished stream."""
+    import threading
+    from sarbp_b200 import _lib
+    hj = pool[3]
+    d = hj.data
+    chunks = [(q, min(48, hj.P - q)) for q in range(0, hj.P, 48)]
+    srv = sb.Server(ctx, hbm_cap_bytes=8e9, lanes=2, max_batch=8, precision=sb.PREC_PRECISE)
+    try:
+        out1 = hj.new_outputs()[0]
+        sid = srv.open_stream(hj.job(out1, precision=sb.PREC_PRECISE), 48)
+        for q0, n in chunks:
+            srv.stream_add(sid, q0, d["phs"][q0:q0 + n])
+        srv.stream_finish(sid)
+
+        out2 = hj.new_outputs()[0]
+        sid = srv.open_stream(hj.job(out2, precision=sb.PREC_PRECISE), 48)
+        errors = []
+
+        def worker(part):
+            try:
+                for q0, n in part:
+                    srv.stream_add(sid, q0, d["phs"][q0:q0 + n])
+            except Exception as exc:  # reported below
+                errors.append(exc)
+
+        threads = [threading.Thread(target=worker, args=(chunks[k::2],)) for k in range(2)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        assert not errors
+        srv.stream_finish(sid)
+        assert rel_l2(out2, out1) < 1e-6
+
+        # an add racing the finish: lands first (then the finish sees one
+        # pulse chunk missing) or is refused as a finished stream
+        out3 = hj.new_outputs()[0]
+        sid = srv.open_stream(hj.job(out3, precision=sb.PREC_PRECISE), 48)
+        for q0, n in chunks[:-1]:
+            srv.stream_add(sid, q0, d["phs"][q0:q0 + n])
+        q0, n = chunks[-1]
+        codes = []
+
+        def late_add():
+            try:
+                srv.stream_add(sid, q0, d["phs"][q0:q0 + n])
+                codes.append(0)
+            except sb.SarbpError as exc:
+                codes.append(exc.code)
+
+        t = threading.Thread(target=late_add)
+        t.start()
+        try:
+            srv.stream_finish(sid)
+            fin = 0
+        except sb.SarbpError as exc:
+            fin = exc.code
+        t.join()
+        assert (codes, fin) in (([0], 0), ([_lib.ERR_INVALID], _lib.ERR_STATE))
+        if fin == 0:
+            assert np.array_equal(out3, out1) or rel_l2(out3, out1) < 1e-6
+        assert srv.stats()["in_use_bytes"] == 0
+    finally:
+        srv.close()
