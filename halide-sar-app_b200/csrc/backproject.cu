@@ -129,8 +129,13 @@ __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
 // One pulse (record rec, window at byte offset poff) for a consumer's pixel
 // pairs.  The sine and cosine are written straight into the pair registers
-// that the accumulation's f32x2 FMAs read.
-template <int MODE, bool PLANAR, bool WIDE, int NP>
+// that the accumulation's f32x2 FMAs read.  PRE: the series products e^2
+// and e - e' come from the record's fourth float4 (formed by the producer)
+// instead of being formed per pulse here; the same f32 products either way.
+// Kernels at 3 CTAs per SM take them from the record (0.9 % faster at
+// 2048^2 x 1999 by register assignment), those at 2 form them (batches of
+// uneven jobs, where the extra shared load cost as much as it saved).
+template <int MODE, bool PLANAR, bool WIDE, int NP, bool PRE>
 __device__ __forceinline__ void pulse_step(const float4 *__restrict__ rec, uint32_t poff, float2 ILK, float2 CL,
                                            const float2 (&dx)[NP], const float2 (&dy)[NP],
                                            const float2 (&dz)[NP], const float2 (&nd2)[NP],
@@ -142,11 +147,21 @@ __device__ __forceinline__ void pulse_step(const float4 *__restrict__ rec, uint3
     const float2 AX = f2(q0.x, q0.y), AY = f2(q0.z, q0.w), AZ = f2(q1.x, q1.y);
     const float2 E = f2(q1.z, q1.w), C0 = f2(q2.x, q2.y), B = f2(q2.z, q2.w);
     float Rp = 0.0f;
-    if constexpr (MODE == 3) Rp = rec[3].x;
-    const float ee = q1.z * q1.z;
-    const float2 EE = f2(ee);
-    const float de = -4.0f * ee * q2.z;  // e - e' (narrow tiles)
-    const float2 DE = f2(de);
+    float2 EE = f2(0.0f), DE = f2(0.0f);
+    if constexpr (PRE) {
+        if constexpr (MODE >= 1) {
+            const float4 q3 = rec[3];  // (e^2, e^2, e - e', e - e'), or (k_c R, 0, ...) in mode 3
+            DE = f2(q3.z, q3.w);
+            if constexpr (MODE == 3) Rp = q3.x;
+            else EE = f2(q3.x, q3.y);
+        }
+    } else {
+        if constexpr (MODE == 3) Rp = rec[3].x;
+        const float ee = q1.z * q1.z;
+        EE = f2(ee);
+        const float de = -4.0f * ee * q2.z;  // e - e' (narrow tiles)
+        DE = f2(de);
+    }
 #pragma unroll
     for (int j = 0; j < NP; ++j) {
         float2 D, s;  // phase argument; s = w_hat . d (approximate for narrow tiles)
@@ -218,7 +233,7 @@ __device__ __forceinline__ void pulse_step(const float4 *__restrict__ rec, uint3
 
 // Inner loop over the nc pulses of a chunk (records rec2, windows from byte
 // offset poff, pstride bytes apart); CL clamps the bin argument (modes 2, 3).
-template <int MODE, bool PLANAR, bool WIDE, int NP>
+template <int MODE, bool PLANAR, bool WIDE, int NP, bool PRE>
 __device__ __forceinline__ void accumulate(int nc, const float4 *__restrict__ rec2, uint32_t poff,
                                            uint32_t pstride, float2 ILK, float2 CL,
                                            const float2 (&dx)[NP], const float2 (&dy)[NP],
@@ -226,16 +241,16 @@ __device__ __forceinline__ void accumulate(int nc, const float4 *__restrict__ re
                                            const float2 (&s0)[NP], float2 (&ar)[NP], float2 (&ai)[NP]) {
 #pragma unroll 6
     for (int i = 0; i < nc; ++i, poff += pstride)
-        pulse_step<MODE, PLANAR, WIDE, NP>(rec2 + 4 * i, poff, ILK, CL, dx, dy, dz, nd2, s0, ar, ai);
+        pulse_step<MODE, PLANAR, WIDE, NP, PRE>(rec2 + 4 * i, poff, ILK, CL, dx, dy, dz, nd2, s0, ar, ai);
 }
 
-template <bool WIDE, int NP>
+template <bool WIDE, int NP, bool PRE>
 __device__ __forceinline__ void accumulate_mode(int mode, bool planar, int nc, const float4 *rec2,
                                                 uint32_t poff, uint32_t pstride, float2 ILK, float2 CL,
                                                 const float2 (&dx)[NP], const float2 (&dy)[NP],
                                                 const float2 (&dz)[NP], const float2 (&nd2)[NP],
                                                 const float2 (&s0)[NP], float2 (&ar)[NP], float2 (&ai)[NP]) {
-#define SARBP_ACC(M, PL) accumulate<M, PL, WIDE, NP>(nc, rec2, poff, pstride, ILK, CL, dx, dy, dz, nd2, s0, ar, ai)
+#define SARBP_ACC(M, PL) accumulate<M, PL, WIDE, NP, PRE>(nc, rec2, poff, pstride, ILK, CL, dx, dy, dz, nd2, s0, ar, ai)
     if (mode == 0) {
         if (planar) SARBP_ACC(0, true);
         else SARBP_ACC(0, false);
@@ -294,15 +309,6 @@ __device__ __forceinline__ bool stage_chunk(const DevJob &jb, int tile, int lane
     }
     bool ok = mbar_wait(&sm.mbar_rec[b], uses[b] & 1u);
     uses[b]++;
-    // records as the consumers read them: four float4 of broadcast pairs
-    float4 *r2 = sm.rec2 + (size_t)b * 4 * cmax;
-    for (int i = lane; i < nc; i += 32) {
-        const float4 a = rec[i].a, q = rec[i].b;
-        r2[4 * i] = make_float4(a.x, a.x, a.y, a.y);
-        r2[4 * i + 1] = make_float4(a.z, a.z, a.w, a.w);
-        r2[4 * i + 2] = make_float4(q.x, q.x, q.y, q.y);
-        r2[4 * i + 3] = make_float4(q.z, q.w, 0.0f, 0.0f);
-    }
     // window copies: bins [base, base + W) of row p; the in-profile part
     // [max(base, 0), min(base + W, N)) comes from the pairs row
     uint32_t bytes = 0;
@@ -318,6 +324,19 @@ __device__ __forceinline__ bool stage_chunk(const DevJob &jb, int tile, int lane
     for (int o = 16; o > 0; o >>= 1) {
         bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
         mode = max(mode, __shfl_xor_sync(0xffffffffu, mode, o));
+    }
+    // records as the consumers read them: four float4 of broadcast pairs;
+    // the fourth holds the per-pulse products of the series terms (e^2 and
+    // e - e' = -4 e^2 sigma0), or k_c R for the closed form (mode 3)
+    float4 *r2 = sm.rec2 + (size_t)b * 4 * cmax;
+    for (int i = lane; i < nc; i += 32) {
+        const float4 a = rec[i].a, q = rec[i].b;
+        r2[4 * i] = make_float4(a.x, a.x, a.y, a.y);
+        r2[4 * i + 1] = make_float4(a.z, a.z, a.w, a.w);
+        r2[4 * i + 2] = make_float4(q.x, q.x, q.y, q.y);
+        const float ee = a.w * a.w;
+        const float de = -4.0f * ee * q.y;
+        r2[4 * i + 3] = mode == 3 ? make_float4(q.z, 0.0f, de, de) : make_float4(ee, ee, de, de);
     }
     if (lane == 0) {
         sm.s_mode[b] = mode;
@@ -377,7 +396,7 @@ __device__ __forceinline__ void producer_loop(const DevJob *__restrict__ jobs,
     }
 }
 
-template <int TX, int TY>
+template <int TX, int TY, bool PRE>
 __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
                                               const WorkItem *__restrict__ items, int nitems,
                                               int *__restrict__ counter, int stage_cap, int cmax,
@@ -476,10 +495,10 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
                 const int nc = min(sh.C, P - p0);
                 const float4 *rec2 = sm.rec2 + (size_t)b * 4 * cmax;
                 if (ti.wide)
-                    accumulate_mode<true, NP>(sm.s_mode[b], ti.planar != 0, nc, rec2, poff, pstride, ILK, CL,
+                    accumulate_mode<true, NP, PRE>(sm.s_mode[b], ti.planar != 0, nc, rec2, poff, pstride, ILK, CL,
                                               dxp, dyp, dzp, nd2p, s0p, arp, aip);
                 else
-                    accumulate_mode<false, NP>(sm.s_mode[b], ti.planar != 0, nc, rec2, poff, pstride, ILK, CL,
+                    accumulate_mode<false, NP, PRE>(sm.s_mode[b], ti.planar != 0, nc, rec2, poff, pstride, ILK, CL,
                                                dxp, dyp, dzp, nd2p, s0p, arp, aip);
                 bar_arrive(kBarEmpty0 + b);
             }
@@ -557,7 +576,7 @@ __global__ void __launch_bounds__(kThreads, MINB) bp_tile_kernel(const DevJob *_
     if (__shfl_sync(0xffffffffu, (int)threadIdx.x, 0) >= kConsumers)
         producer_loop(jobs, items, nitems, stage_cap, cmax, persistent, sm);
     else
-        consumer_loop<TX, TY>(jobs, items, nitems, counter, stage_cap, cmax, persistent, sm);
+        consumer_loop<TX, TY, (MINB >= 3)>(jobs, items, nitems, counter, stage_cap, cmax, persistent, sm);
 }
 
 // ---- naive FP32 kernel: one thread per pixel ----
