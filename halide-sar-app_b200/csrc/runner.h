@@ -136,6 +136,10 @@ private:
     PinnedBuffer host_meta_;
     cudaEvent_t meta_done_ = nullptr;  // host_meta_ may be rewritten after this
     cudaEvent_t front_done_ = nullptr; // range compression done (slabbed runs)
+    // Range compression runs on side_ beside the tile geometry on the main
+    // stream (both only read the set-up's tables); fork_/join_ order them.
+    cudaStream_t side_ = nullptr;
+    cudaEvent_t fork_ = nullptr, join_ = nullptr;
     int last_njobs_ = 0;
     PinnedBuffer status_pin_;          // JobScalars of the last batch, copied behind it
     cudaMemPool_t pool_ = nullptr;
