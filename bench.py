@@ -25,6 +25,7 @@ bounded pixel sample of the same workload; only rank 0 runs it.
 import argparse
 import json
 import os
+import math
 import statistics
 import subprocess
 import sys
@@ -67,6 +68,10 @@ def parse():
     ap.add_argument("--njobs", type=int, default=96, help="batch96: number of jobs")
     ap.add_argument("--no-autotune", action="store_true",
                     help="batch96: use --tile/--chunk/--min-blocks/--stage-cap instead of the autotuner")
+    ap.add_argument("--per-job", action="store_true",
+                    help="batch96: time every job alone instead (per-job rates by tile regime)")
+    ap.add_argument("--only-job", type=int, default=-1,
+                    help="batch96: run job J alone --steps times and exit (profiling one job)")
     ap.add_argument("--serve-rates", default="20,50,100,200,400", help="serve: arrival rates (req/s)")
     ap.add_argument("--serve-requests", type=int, default=2000, help="serve: requests per rate")
     ap.add_argument("--serve-lanes", type=int, default=3, help="serve: concurrent batches")
@@ -663,6 +668,12 @@ def run_batch(args, rank, world, local_rank):
             ms = float(t.item())
         return ms
 
+    if args.per_job or args.only_job >= 0:
+        r = per_job_measure(torch, ctx, stream, dev, args.njobs, 7 + rank, args.only_job, args.steps)
+        ctx.close()
+        if rank == 0 and r is not None:
+            print(json.dumps(r), flush=True)
+        return
     tune = None
     if args.no_autotune:
         tune = dict(tile=tuple(int(x) for x in (args.tile or "32x32").split("x")),
@@ -690,6 +701,53 @@ def run_batch(args, rank, world, local_rank):
     }
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def per_job_measure(torch, ctx, stream, dev, njobs, seed, only, steps):
+    """Each batch96 job alone through the device entry point (default launch
+    shape): its backprojection ms from the library's stage events, with the
+    job's tile regime (k_c x 32x32-tile half-diagonal: wide above 1024 rad;
+    gm = half-diagonal / 2 R0, which sets the series order).  With `only`,
+    runs that one job `steps` times and returns None (a profiling target)."""
+    import sarbp_b200 as sb
+    from sarbp_b200 import synth
+    from sarbp_b200.batch import DeviceJob
+    cfgs = synth.batch_jobs(njobs=njobs, seed=seed)
+    if only >= 0:
+        j = DeviceJob(cfgs[only], torch, dev)
+        for _ in range(max(1, steps)):
+            ctx.run_jobs([j.job])
+        ctx.synchronize()
+        return None
+    c_light = 299792458.0
+    rows = []
+    for i, c in enumerate(cfgs):
+        j = DeviceJob(c, torch, dev)
+        for _ in range(2):
+            ctx.run_jobs([j.job])
+        ctx.set_timing(True)
+        st = []
+        for _ in range(3):
+            ctx.run_jobs([j.job])
+            st.append(ctx.last_stage_ms())
+        ctx.set_timing(False)
+        ctx.synchronize()
+        bp = float(np.median(np.array(st), axis=0)[3])
+        rho = 16 * math.sqrt(2) * c["extent"] / c["n"]
+        kc = 4 * math.pi * (c["f0"] + c["S"] / 2 * c["df"]) / c_light
+        rows.append({"job": i, "n": c["n"], "P": c["P"], "S": c["S"], "kc_rho": kc * rho,
+                     "gm": rho / (2 * c["R0"]), "bp_ms": bp, "rate": c["n"] ** 2 * c["P"] / (bp * 1e-3) / 1e9})
+        del j
+    groups = {}
+    for r in rows:
+        key = "%d^2 %s" % (r["n"], "wide" if r["kc_rho"] > 1024 else "narrow")
+        g = groups.setdefault(key, [0, 0.0, 0.0])
+        g[0] += 1
+        g[1] += r["n"] ** 2 * r["P"]
+        g[2] += r["bp_ms"]
+    return {"metric": "Gpixel*pulses/s of each batch96 job alone (backprojection stage)",
+            "by_regime": {k: {"jobs": g[0], "rate": g[1] / (g[2] * 1e-3) / 1e9} for k, g in sorted(groups.items())},
+            "sum_alone_ms": sum(r["bp_ms"] for r in rows), "jobs": rows}
 
 
 def fp64_sample_rel_l2(pool, picks, seed, pixels=1000):
