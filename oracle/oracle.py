@@ -53,6 +53,8 @@ def lib():
         L.orc_range_compress.argtypes = [_fp, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int]
         L.orc_norm_r0.argtypes = [_dp, ctypes.c_int, ctypes.c_int, _dp]
+        L.orc_interp_linspace.argtypes = [_dp, ctypes.c_longlong, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_int, _dp, _dp]
         L.orc_backproject.argtypes = [
             _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp,
             ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong), ctypes.c_longlong,
@@ -159,6 +161,17 @@ def fft_forward(x):
     a = np.ascontiguousarray(x, np.complex128).copy()
     lib().orc_fft_forward(a.view(np.float64).ctypes.data_as(_dp), a.size)
     return a
+
+
+def interp_linspace(xs, lsa, lsb, lsn, fp):
+    """The interp of backprojection.cpp:52-65: complex fp sampled on
+    linspace(lsa, lsb, lsn), evaluated at xs (clamped like the reference)."""
+    xs = np.ascontiguousarray(xs, np.float64)
+    q = np.ascontiguousarray(np.asarray(fp, np.complex128)).view(np.float64)
+    out = np.zeros(2 * xs.size, np.float64)
+    lib().orc_interp_linspace(_ptr(xs, ctypes.c_double), xs.size, float(lsa), float(lsb), int(lsn),
+                              _ptr(q, ctypes.c_double), _ptr(out, ctypes.c_double))
+    return out.view(np.complex128)
 
 
 def range_compress(phs, k_r, taylor_s_l, n_fft, mode=MODE_REF, nthreads=0, taylor_mode=0):

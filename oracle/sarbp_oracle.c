@@ -397,6 +397,32 @@ static inline double dr_at(const double *pp, double nr0, double rx, double ry,
 }
 
 /*
+ * The interp of backprojection.cpp:52-65 on a linspace axis: t = (x - lsa)
+ * / lsr, lower index floor(t), both indices clamped to [0, n-1] and the
+ * offset to [0, 1], lerp of the complex samples q ([n][2]).
+ */
+static inline void interp_at(const double *q, long long n, double t, double *qr, double *qi) {
+    if (!(t > -1e9)) t = -1e9; /* keep the int conversion defined */
+    if (t > 1e9) t = 1e9;
+    double fl = floor(t);
+    long long l = (long long)fl;
+    double fr = t - (double)l;
+    long long cl = l < 0 ? 0 : (l > n - 1 ? n - 1 : l);
+    long long cu = l + 1 < 0 ? 0 : (l + 1 > n - 1 ? n - 1 : l + 1);
+    if (fr < 0.0) fr = 0.0;
+    if (fr > 1.0) fr = 1.0;
+    *qr = q[2 * cl] * (1.0 - fr) + q[2 * cu] * fr;
+    *qi = q[2 * cl + 1] * (1.0 - fr) + q[2 * cu + 1] * fr;
+}
+
+void orc_interp_linspace(const double *xs, long long nx, double lsa, double lsb, int lsn,
+                         const double *q, double *out) {
+    double lsr = (lsb - lsa) / (double)(lsn - 1);
+    for (long long i = 0; i < nx; i++)
+        interp_at(q, lsn, (xs[i] - lsa) / lsr, &out[2 * i], &out[2 * i + 1]);
+}
+
+/*
  * backprojection.cpp:110-138 and the interp of :52-65:
  *   dr    = norm_r0(p) - |r(pix) - pos(p)|
  *   t     = (dr - lsa) / lsr, lsa = floor(-S*dr/2), lsb = floor(S*dr/2),
@@ -444,18 +470,8 @@ int orc_backproject(const double *Q, int P, int N, int S, double delta_r,
             for (int k = 0; k < nv4; k++) {
                 long long i = pix[k];
                 double dr = dr_at(pp, nr0[p], rx[i], ry[i], rz[i]);
-                double t = (dr - lsa) / lsr;
-                if (!(t > -1e9)) t = -1e9; /* keep the int conversion defined */
-                if (t > 1e9) t = 1e9;
-                double fl = floor(t);
-                long long l = (long long)fl;
-                double fr = t - (double)l;
-                long long cl = l < 0 ? 0 : (l > N - 1 ? N - 1 : l);
-                long long cu = l + 1 < 0 ? 0 : (l + 1 > N - 1 ? N - 1 : l + 1);
-                if (fr < 0.0) fr = 0.0;
-                if (fr > 1.0) fr = 1.0;
-                double qr = q[2 * cl] * (1.0 - fr) + q[2 * cu] * fr;
-                double qi = q[2 * cl + 1] * (1.0 - fr) + q[2 * cu + 1] * fr;
+                double qr, qi;
+                interp_at(q, N, (dr - lsa) / lsr, &qr, &qi);
                 double ph = (-k_c) * dr;
                 double s, c;
                 sincos(ph, &s, &c);

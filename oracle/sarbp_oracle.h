@@ -72,6 +72,10 @@ int orc_range_compress(const float *phs, int S, int P, const double *k_r,
  * the op order (x*x + y*y) + z*z, no fused multiply-add; f64 in FP64 mode.
  * pos is f64 [P][3] (in REF mode its values are first rounded to f32). */
 void orc_norm_r0(const double *pos, int P, int mode, double *nr0);
+/* backprojection.cpp:52-65: complex samples q[lsn][2] on linspace(lsa, lsb,
+ * lsn), interpolated at xs[nx] with the reference's clamps -> out[nx][2]. */
+void orc_interp_linspace(const double *xs, long long nx, double lsa, double lsb, int lsn,
+                         const double *q, double *out);
 
 /* Per-pixel pulse accumulation, backprojection.cpp:110-138.  Evaluates the
  * output image at the n_out output pixels listed in out_idx (y*nu + x, in

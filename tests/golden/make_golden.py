@@ -7,7 +7,8 @@ Writes
   reference_known_answers.json  known-answer values of the reference's own
                                 unit tests (test/taylor_test.cpp,
                                 test/norm_test.cpp, test/cross_test.cpp,
-                                test/linspace_test.cpp, test/arange_test.cpp),
+                                test/linspace_test.cpp, test/arange_test.cpp,
+                                test/interp_test.cpp),
                                 parsed from the test sources
   afrl_img_plane.npz            RITSAR image-plane outputs for AFRL pass 1
                                 (data/AFRL/pass1/HH_ip_npy/*.npy)
@@ -81,6 +82,13 @@ def known_answers(ref):
     out["arange"] = {"start": start, "stop": stop, "step": step, "expected": listed,
                      "tol": float(re.search(r">=\s*([\d.]+)f", src).group(1)),
                      "source": "test/arange_test.cpp:18-40"}
+
+    src = _read(ref, "test/interp_test.cpp")
+    arr = lambda name: _floats(re.search(r"float %s\[\w+\]\s*=\s*\{([^}]*)\}" % name, src).group(1))
+    out["interp"] = {"xs": arr("xs"), "xp": arr("xp"), "fp": arr("fp"),
+                     "expected": _floats(re.search(r"output should be:\s*\[([^\]]*)\]", src).group(1)),
+                     "tol": float(re.search(r">=\s*([\d.]+)f", src).group(1)),
+                     "source": "test/interp_test.cpp:15-26"}
     return out
 
 

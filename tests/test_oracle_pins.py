@@ -52,6 +52,21 @@ def test_linspace(oracle, known_answers):
     assert out[-1] == np.float32(ka["stop"]) and out[0] == np.float32(ka["start"])
 
 
+def test_interp_known_answer(oracle, known_answers):
+    """The linspace interpolation of backprojection.cpp:52-65 (clamped below
+    the first and above the last sample) against the reference's interp
+    known answers (test/interp_test.cpp:15-26), on the real and imaginary
+    parts."""
+    ka = known_answers["interp"]
+    xp = np.array(ka["xp"])
+    assert np.allclose(np.diff(xp), xp[1] - xp[0])  # a linspace axis
+    fp = np.array(ka["fp"])
+    out = oracle.interp_linspace(ka["xs"], xp[0], xp[-1], xp.size, fp - 2j * fp)
+    exp = np.array(ka["expected"])
+    assert np.all(np.abs(out.real - exp) < ka["tol"])
+    assert np.all(np.abs(out.imag + 2 * exp) < 2 * ka["tol"])
+
+
 def test_arange(oracle, known_answers):
     ka = known_answers["arange"]  # test/arange_test.cpp:18-40
     n = int(np.ceil((ka["stop"] - ka["start"]) / ka["step"]))
