@@ -164,6 +164,48 @@ def test_plain_large_full_size_sampled(ctx, oracle):
     assert np.all(np.isfinite(img))
 
 
+def test_largest_image_32768_squared_sampled(sb, torch, oracle):
+    """A 32768^2 image (2^30 pixels, the size of the reference's largest
+    Sandia runs) from plain_large's aperture in one device call on one GPU:
+    pixel positions from the image-plane axes, the 17 GB image and ~75 GB
+    of scratch on the device (its own context, released afterwards); 4096
+    sampled pixels against the oracle at the reference's precision."""
+    from sarbp_b200 import synth
+    d = synth.make("plain_large", seed=4, with_r=False, overrides=dict(n=32768, extent=200.0))
+    nu, nv = d["nu"], d["nv"]
+    assert nu * nv == 1 << 30
+    dev = torch.device("cuda", 0)
+    pos32, k32 = d["pos"].astype(np.float32), d["k_r"].astype(np.float32)
+    c = sb.Context(0)
+    try:
+        t = dict(phs=torch.from_numpy(d["phs"].view(np.float32).copy()).to(dev), k=torch.from_numpy(k32).to(dev),
+                 pos=torch.from_numpy(pos32).to(dev), u=torch.from_numpy(d["u"]).to(dev),
+                 v=torch.from_numpy(d["v"]).to(dev))
+        out = torch.empty((nv, nu, 2), dtype=torch.float64, device=dev)
+        job = sb.make_job(d["S"], d["P"], d["N_fft"], d["taylor"], nu, nv, d["delta_r"], t["phs"].data_ptr(),
+                          t["k"].data_ptr(), t["pos"].data_ptr(), out.data_ptr(), u=t["u"].data_ptr(),
+                          v=t["v"].data_ptr(), u_hat=d["u_hat"], v_hat=d["v_hat"])
+        c.run_jobs([job])
+        c.synchronize()
+        rng = np.random.default_rng(5)
+        ix, iy = rng.integers(0, nu, 4096), rng.integers(0, nv, 4096)
+        rows = torch.from_numpy(nv - 1 - iy).to(dev)
+        got = out[rows, torch.from_numpy(ix).to(dev)].cpu().numpy().view(np.complex128)[:, 0]
+        del out, t
+    finally:
+        c.close()
+        torch.cuda.empty_cache()
+    # the sampled pixels' positions as img_plane.cpp:92-102 forms them
+    uh, vh = np.asarray(d["u_hat"], np.float64), np.asarray(d["v_hat"], np.float64)
+    r = np.stack([(uh[k] * d["u"][ix]) + (vh[k] * d["v"][iy]) for k in range(3)])
+    ref = oracle.backproject(oracle.range_compress(d["phs"], k32, d["taylor"], d["N_fft"]), d["S"],
+                             d["delta_r"], k32, pos32, r, r.shape[1], 1)[0]
+    e = rel_l2(got, ref)
+    print("32768^2 sampled rel-L2 %.3e" % e)
+    assert e < REL_COMPAT
+    assert np.all(np.isfinite(got))
+
+
 def test_linearity_full_size(ctx):
     """BP(a x + b y) = a BP(x) + b BP(y) at plain_large size."""
     from sarbp_b200 import synth
