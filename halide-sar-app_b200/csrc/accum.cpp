@@ -42,8 +42,15 @@ namespace {
 size_t a256(size_t x) { return (x + 255) / 256 * 256; }
 
 struct AccumLayout {
-    size_t sc, job, items, rows, cnt, filt, wS, wP, pulse, tiles, fin, acc, Qp, recs, pulse_c, wP_c, end;
+    size_t sc, job, items, rows, cnt, filt, wS, wP, pulse, tiles, fin, acc, Qp, recs, pulse_c, wP_c, work, end;
+    int work_rows;  // rows of the four-step range compression's work buffer (0: none)
 };
+
+int log2_of(int n) {
+    int l = 0;
+    while ((1 << l) < n) ++l;
+    return l;
+}
 
 AccumLayout accum_layout(const sarbp_job &j, int tile_x, int tile_y, int C) {
     const size_t P = (size_t)j.npulses, S = (size_t)j.nsamples, N = (size_t)j.n_fft;
@@ -67,6 +74,9 @@ AccumLayout accum_layout(const sarbp_job &j, int tile_x, int tile_y, int C) {
     L.recs = o;    o = a256(o + ntiles * (size_t)C * sizeof(PulseRec));
     L.pulse_c = o; o = a256(o + (size_t)C * sizeof(double4));
     L.wP_c = o;    o = a256(o + (size_t)C * sizeof(float));
+    const int logN = log2_of(j.n_fft);
+    L.work_rows = logN > kMaxLogNSmem ? std::min(C, rc_work_rows(logN)) : 0;
+    L.work = o;    o = a256(o + (size_t)L.work_rows * N * sizeof(float2));
     L.end = o;
     return L;
 }
@@ -113,7 +123,6 @@ struct sarbp_accum {
     DeviceBuffer stage;  // two staging buffers of C phase-history rows (host path)
     PinnedBuffer status_pin;
     DevJob base{};       // host copy of the whole job's descriptor
-    const float2 *tw = nullptr;
     std::vector<unsigned char> added;
     long long nadded = 0;
     long long nhost = 0;  // host-path chunks so far
@@ -198,7 +207,9 @@ int sarbp_accum::add(int q0, int n, const float *phs_rows, cudaEvent_t rc_done) 
     int *cnt = reinterpret_cast<int *>(dptr(lay.cnt));
     cudaError_t e = launch_chunk_tables(base.pulse, base.wP, P, q0, n, c.pulse, c.wP, s);
     if (e == cudaSuccess) e = launch_store_job(c, d_job(), s);
-    if (e == cudaSuccess) e = launch_range_compress(logN, d_job(), rows, n, 1, tw, s);
+    if (e == cudaSuccess)
+        e = range_compress_rows(&ctx->dev, logN, d_job(), rows, n, 1, reinterpret_cast<float2 *>(dptr(lay.work)),
+                                lay.work_rows, s);
     if (e == cudaSuccess && rc_done) e = cudaEventRecord(rc_done, s);
     if (e == cudaSuccess) e = launch_tile_records(d_job(), items, ntiles, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, sizeof(int), s);
@@ -247,10 +258,12 @@ int sarbp::accum_create_on(sarbp_ctx *ctx, const sarbp_job *job, const sarbp_opt
     a->added.assign(a->P, 0);
     cudaError_t e = a->mem.alloc_exact(a->lay.end);
     if (e != cudaSuccess) return cuda_fail(e, "pulse-chunked job: device memory");
+    // the twiddle tables now (one-time synchronous uploads), not at an add
     float2 *tw = nullptr;
     e = ctx->dev.twiddle(a->logN, &tw);
+    if (e == cudaSuccess && a->logN > kMaxLogNSmem) e = ctx->dev.twiddle(a->logN / 2, &tw);
+    if (e == cudaSuccess && a->logN > kMaxLogNSmem) e = ctx->dev.twiddle(a->logN - a->logN / 2, &tw);
     if (e != cudaSuccess) return cuda_fail(e, "twiddle table");
-    a->tw = tw;
     e = a->status_pin.ensure(sizeof(JobScalars));
     if (e != cudaSuccess) return cuda_fail(e, "pinned status word");
     for (int b = 0; b < 2 && e == cudaSuccess; ++b) {

@@ -13,8 +13,9 @@
 namespace sarbp {
 
 constexpr int kMaxTaylorTerms = 64;  // n_bar - 1 <= 64  (S_L up to ~150 dB)
-constexpr int kMinLogN = 4;          // N_fft in [16, 16384]
-constexpr int kMaxLogN = 14;
+constexpr int kMinLogN = 4;          // N_fft in [16, 131072]
+constexpr int kMaxLogN = 17;
+constexpr int kMaxLogNSmem = 14;     // up to here one CTA holds a whole row
 
 // status bits written by kernels into JobScalars::status
 constexpr int kStatusTileTooWide = 1;   // range window of a tile exceeds smem

@@ -21,6 +21,16 @@ void fill_twiddle_table(int logN, float2 *host);
 cudaError_t launch_range_compress(int logN, const DevJob *d_jobs, const RowItem *d_rows, int nrows, int pairs,
                                   const float2 *d_tw, cudaStream_t st);
 cudaError_t init_range_compress_attributes();
+// N_fft above 2^kMaxLogNSmem: a four-step FFT through `work`, which holds
+// work_rows rows of N_fft complex values (rows go through it work_rows at a
+// time; rc_work_rows(logN) rows, rc_work_bytes(logN) bytes, is about
+// 256 MB); tw1 and tw2 are the tables of logN / 2 and logN - logN / 2, twN
+// the W_N table.
+int rc_work_rows(int logN);
+size_t rc_work_bytes(int logN);
+cudaError_t launch_range_compress_large(int logN, const DevJob *d_jobs, const RowItem *d_rows, int nrows,
+                                        int pairs, const float2 *tw1, const float2 *tw2, const float2 *twN,
+                                        float2 *work, int work_rows, cudaStream_t st);
 
 // backproject.cu
 struct BpLaunch {

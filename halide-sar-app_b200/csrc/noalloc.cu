@@ -48,7 +48,7 @@ constexpr int kMaxDevices = 64;
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-// Fixed offsets of the twiddle tables of logN = kMinLogN..kMaxLogN at the
+// Fixed offsets of the twiddle tables of logN = kMinLogN..kMaxLogNSmem at the
 // start of the scratch (256-byte aligned each).
 constexpr size_t twiddle_offset(int logN) {
     size_t o = 0;
@@ -60,7 +60,7 @@ constexpr size_t twiddle_offset(int logN) {
     }
     return o;
 }
-constexpr size_t kTwiddleBytes = twiddle_offset(kMaxLogN + 1);
+constexpr size_t kTwiddleBytes = twiddle_offset(kMaxLogNSmem + 1);
 
 // The scratch.  Host code must not use this symbol as an address: the device
 // address comes from cudaGetSymbolAddress below.
@@ -102,7 +102,7 @@ int scratch_for_device(int dev, cudaStream_t st, void **addr, int *num_sms) {
         e = init_range_compress_attributes();
         if (e == cudaSuccess) e = init_backproject_attributes();
         if (e != cudaSuccess) return cuda_fail(e, "setting kernel attributes");
-        for (int l = kMinLogN; l <= kMaxLogN; ++l)
+        for (int l = kMinLogN; l <= kMaxLogNSmem; ++l)
             twiddle_kernel<<<64, 256, 0, st>>>(reinterpret_cast<float2 *>(static_cast<char *>(p) +
                                                                           twiddle_offset(l)), l);
         e = cudaGetLastError();
@@ -143,7 +143,7 @@ extern "C" int sarbp_backprojection_noalloc(const sarbp_job *job, void *cuda_str
     auto bad = [](const char *what) { return fail(SARBP_ERR_INVALID, std::string("no-alloc: ") + what); };
     if (j.nsamples < 1 || j.npulses < 1 || j.nu < 1 || j.nv < 1) return bad("sizes must be >= 1");
     if ((long long)j.nu * j.nv > (1ll << 31)) return bad("image larger than 2^31 pixels");
-    if (j.n_fft < (1 << kMinLogN) || j.n_fft > (1 << kMaxLogN) || (j.n_fft & (j.n_fft - 1)))
+    if (j.n_fft < (1 << kMinLogN) || j.n_fft > (1 << kMaxLogNSmem) || (j.n_fft & (j.n_fft - 1)))
         return fail(SARBP_ERR_UNSUPPORTED, "no-alloc: N_fft must be a power of two in [16, 16384]");
     if (prec != SARBP_PREC_COMPAT && prec != SARBP_PREC_PRECISE)
         return bad("precision must be SARBP_PREC_COMPAT or SARBP_PREC_PRECISE");

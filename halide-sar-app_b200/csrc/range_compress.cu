@@ -246,12 +246,196 @@ range_compress_kernel(const DevJob *__restrict__ jobs, const RowItem *__restrict
     }
 }
 
+// ---- N_fft above 2^kMaxLogNSmem: four-step FFT through a work buffer ----
+// With N = N1 N2, n = N2 n1 + n2 and k = k1 + N1 k2 (Cooley-Tukey):
+//   Y[n2][k1]     = W_N^(n2 k1) * DFT_N1 over n1 of x[N2 n1 + n2]  (columns)
+//   X[k1 + N1 k2] = DFT_N2 over n2 of Y[n2][k1]                     (rows)
+// The columns kernel writes Y to work[row][k1][n2]; the rows kernel stores
+// with the fftshift, Q[j] = X[(j + N/2) mod N] at j = k1 + N1 k2',
+// k2' = (k2 + N2/2) mod N2.  Both sub-DFTs run the radix-16 passes above on
+// rows of shared memory, one CTA holding several columns (stride STR, one
+// float2 more than a padded row so that neighbouring columns fall in other
+// banks).
+
+// The passes of one sub-DFT; on return thread t holds X[t + r N/16] in v[r].
+template <int N, int NS>
+__device__ __forceinline__ void passes16_regs(float2 (&v)[16], int t, float2 *sm, const float2 *tw_base,
+                                              int tw_off) {
+    pass_compute<N, 16, NS>(v, t, tw_base + tw_off);
+    if constexpr (NS * 16 < N) {
+        __syncthreads();
+        pass_store_smem<N, 16, NS>(v, t, sm);
+        __syncthreads();
+        pass_load_smem<N, 16>(v, t, sm);
+        passes16_regs<N, NS * 16>(v, t, sm, tw_base, tw_off + (NS > 1 ? 15 * NS : 0));
+    }
+}
+
+// Loads a sub-DFT's first-pass inputs from its shared row (as the single-row
+// kernel loads them from global memory) and runs all passes.
+template <int N>
+__device__ __forceinline__ void fft_row_regs(float2 (&v)[16], int t, float2 *sm, const float2 *tw) {
+    constexpr int T = N / 16, R0 = Plan<N>::R0, R1 = R0 > 1 ? R0 : 16, NB1 = 16 / R1;
+#pragma unroll
+    for (int b = 0; b < NB1; ++b)
+#pragma unroll
+        for (int r = 0; r < R1; ++r) v[b * R1 + r] = sm[pad_idx(t + b * T + r * (N / R1))];
+    if constexpr (R0 > 1) {
+        pass_compute<N, R0, 1>(v, t, tw);
+        __syncthreads();
+        pass_store_smem<N, R0, 1>(v, t, sm);
+        __syncthreads();
+        pass_load_smem<N, 16>(v, t, sm);
+        passes16_regs<N, R0>(v, t, sm, tw, 0);
+    } else {
+        __syncthreads();  // every thread has read its inputs before the first store
+        passes16_regs<N, 1>(v, t, sm, tw, 0);
+    }
+}
+
+template <int L1>
+struct ColsShape {
+    static constexpr int N1 = 1 << L1, T = N1 / 16, C = 256 / T, STR = N1 + N1 / 16 + 1;
+};
+template <int L2>
+struct RowsShape {
+    static constexpr int N2 = 1 << L2, T = N2 / 16, C = 256 / T, STR = N2 + N2 / 16 + 1;
+};
+
+// Columns: one CTA per (row, C consecutive n2); rows [row0, row0 + grid/groups).
+template <int L1>
+__global__ void __launch_bounds__(256)
+rc_cols_kernel(const DevJob *__restrict__ jobs, const RowItem *__restrict__ rows, int row0, int logN,
+               const float2 *__restrict__ tw1, const float2 *__restrict__ twN, float2 *__restrict__ work) {
+    using Sh = ColsShape<L1>;
+    constexpr int N1 = Sh::N1, T = Sh::T, C = Sh::C, STR = Sh::STR;
+    extern __shared__ float2 smem_all[];
+    const int N = 1 << logN, N2 = N >> L1, groups = N2 / C;
+    const int rb = blockIdx.x / groups, n2_0 = (blockIdx.x % groups) * C;
+    const RowItem it = rows[row0 + rb];
+    const DevJob &jb = jobs[it.job];
+    const int S = jb.S, P = jb.P, p = it.pulse;
+    const int pm = P / 2 + P % 2;
+    const int src = jb.chunked ? p : (int)(((long long)p + 2 * pm) % P);
+    const int x_pad = (N - S) >> 1;
+    const float2 *__restrict__ ph = jb.phs + (size_t)src * S;
+    const float wp = jb.wP[src];
+    // window * filter * pad * fftshift of x[N2 n1 + n2], lanes along n2
+    for (int i = threadIdx.x; i < N1 * C; i += blockDim.x) {
+        const int c = i % C, n1 = i / C;
+        const int s = ((n1 * N2 + n2_0 + c + N / 2) & (N - 1)) - x_pad;
+        float2 x = make_float2(0.f, 0.f);
+        if (s >= 0 && s < S) {
+            const float2 a = __ldg(&ph[s]);
+            const float f = __ldg(&jb.filt[s]);
+            const float w = __ldg(&jb.wS[s]) * wp;
+            x = make_float2((a.x * f) * w, (a.y * f) * w);
+        }
+        smem_all[c * STR + pad_idx(n1)] = x;
+    }
+    __syncthreads();
+    const int c = threadIdx.x / T, t = threadIdx.x % T;
+    float2 *sm = smem_all + c * STR;
+    float2 v[16];
+    fft_row_regs<N1>(v, t, sm, tw1);
+    const int n2 = n2_0 + c;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = cmul(v[r], __ldg(&twN[n2 * (t + r * T)]));
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 16; ++r) sm[pad_idx(t + r * T)] = v[r];
+    __syncthreads();
+    float2 *__restrict__ wrow = work + (size_t)rb * N;
+    for (int i = threadIdx.x; i < N1 * C; i += blockDim.x) {
+        const int cc = i % C, k1 = i / C;
+        wrow[(size_t)k1 * N2 + n2_0 + cc] = smem_all[cc * STR + pad_idx(k1)];
+    }
+}
+
+// Rows: one CTA per (row, C consecutive k1), plus the next column k1_0 + C
+// (column 0 after the last group) for the pairs' right neighbours:
+// Q[j + 1] is column k1 + 1 at the same k2', or column 0 at k2' + 1 when
+// k1 = N1 - 1, and Q[N] is read as Q[N - 1] (the reference's clamp).
+template <int L2>
+__global__ void __launch_bounds__(288)
+rc_rows_kernel(const DevJob *__restrict__ jobs, const RowItem *__restrict__ rows, int row0, int logN,
+               const float2 *__restrict__ tw2, const float2 *__restrict__ work, int pairs) {
+    using Sh = RowsShape<L2>;
+    constexpr int N2 = Sh::N2, T = Sh::T, C = Sh::C, STR = Sh::STR;
+    extern __shared__ float2 smem_all[];
+    const int N = 1 << logN, N1 = N >> L2, groups = N1 / C;
+    const int rb = blockIdx.x / groups, k1_0 = (blockIdx.x % groups) * C;
+    const RowItem it = rows[row0 + rb];
+    const DevJob &jb = jobs[it.job];
+    const int p = it.pulse;
+    const float2 *__restrict__ wrow = work + (size_t)rb * N;
+    for (int i = threadIdx.x; i < (C + 1) * N2; i += blockDim.x) {
+        const int c = i / N2, n2 = i % N2;
+        const int k1 = (k1_0 + c) & (N1 - 1);
+        smem_all[c * STR + pad_idx(n2)] = wrow[(size_t)k1 * N2 + n2];
+    }
+    __syncthreads();
+    const int c = threadIdx.x / T, t = threadIdx.x % T;
+    float2 *sm = smem_all + c * STR;
+    float2 v[16];
+    fft_row_regs<N2>(v, t, sm, tw2);
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 16; ++r) sm[pad_idx((t + r * T + N2 / 2) & (N2 - 1))] = v[r];
+    __syncthreads();
+    if (pairs) {
+        float4 *__restrict__ prow = jb.Qp + (size_t)p * (N + 1);
+        for (int i = threadIdx.x; i < C * N2; i += blockDim.x) {
+            const int cc = i % C, k2 = i / C, k1 = k1_0 + cc;
+            const float2 a = smem_all[cc * STR + pad_idx(k2)];
+            float2 b = a;
+            if (k1 + 1 < N1) b = smem_all[(cc + 1) * STR + pad_idx(k2)];
+            else if (k2 + 1 < N2) b = smem_all[C * STR + pad_idx(k2 + 1)];
+            prow[(size_t)k1 + (size_t)N1 * k2] =
+                make_float4(0.5f * (a.x + b.x), 0.5f * (a.y + b.y), b.x - a.x, b.y - a.y);
+        }
+        if (k1_0 == 0 && threadIdx.x == 0) {
+            const float2 a = smem_all[pad_idx(0)];
+            prow[N] = make_float4(a.x, a.y, 0.f, 0.f);
+        }
+    } else {
+        float2 *__restrict__ qrow = jb.Q + (size_t)p * N;
+        for (int i = threadIdx.x; i < C * N2; i += blockDim.x) {
+            const int cc = i % C, k2 = i / C;
+            qrow[(size_t)(k1_0 + cc) + (size_t)N1 * k2] = smem_all[cc * STR + pad_idx(k2)];
+        }
+    }
+}
+
+template <int L1, int L2>
+cudaError_t launch_four_step(int logN, const DevJob *d_jobs, const RowItem *d_rows, int nrows, int pairs,
+                             const float2 *tw1, const float2 *tw2, const float2 *twN, float2 *work,
+                             int rb, cudaStream_t st) {
+    using A = ColsShape<L1>;
+    using B = RowsShape<L2>;
+    static_assert(L1 + L2 >= 15 && (1 << L2) >= A::C && (1 << L1) >= B::C, "four-step split");
+    const size_t smem_a = (size_t)A::C * A::STR * sizeof(float2);
+    const size_t smem_b = (size_t)(B::C + 1) * B::STR * sizeof(float2);
+    for (int r0 = 0; r0 < nrows; r0 += rb) {
+        const int nb = nrows - r0 < rb ? nrows - r0 : rb;
+        rc_cols_kernel<L1><<<nb * ((1 << L2) / A::C), A::C * A::T, smem_a, st>>>(d_jobs, d_rows, r0, logN, tw1,
+                                                                               twN, work);
+        rc_rows_kernel<L2><<<nb * ((1 << L1) / B::C), (B::C + 1) * B::T, smem_b, st>>>(d_jobs, d_rows, r0, logN,
+                                                                                     tw2, work, pairs);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 }  // namespace
 
 // Twiddle table of one N: for each pass with NS > 1, entries
-// W_{NS*R}^{jm*r} at [(r-1)*NS + jm], passes concatenated in order.
+// W_{NS*R}^{jm*r} at [(r-1)*NS + jm], passes concatenated in order.  Above
+// 2^kMaxLogNSmem (four-step FFTs) the table is W_N^m, m in [0, N).
 int twiddle_table_size(int logN) {
     const int N = 1 << logN;
+    if (logN > kMaxLogNSmem) return N;
     const int R0 = 1 << (logN % 4);
     int ns = R0 > 1 ? R0 : 1;
     int total = 0;
@@ -265,6 +449,13 @@ int twiddle_table_size(int logN) {
 
 void fill_twiddle_table(int logN, float2 *host) {
     const int N = 1 << logN;
+    if (logN > kMaxLogNSmem) {
+        for (int m = 0; m < N; ++m) {
+            const double a = -2.0 * 3.14159265358979323846 * (double)m / (double)N;
+            host[m] = make_float2((float)cos(a), (float)sin(a));
+        }
+        return;
+    }
     const int R0 = 1 << (logN % 4);
     int ns = R0 > 1 ? R0 : 16;
     int off = 0;
@@ -318,6 +509,29 @@ cudaError_t init_range_compress_attributes() {
     if (e == cudaSuccess) e = rc_attr<13>();
     if (e == cudaSuccess) e = rc_attr<14>();
     return e;
+}
+
+int rc_work_rows(int logN) {
+    // about 256 MB of work buffer (2^25 complex values)
+    return logN > kMaxLogNSmem ? (logN >= 25 ? 1 : 1 << (25 - logN)) : 0;
+}
+
+size_t rc_work_bytes(int logN) {
+    return logN > kMaxLogNSmem ? (size_t)rc_work_rows(logN) * ((size_t)1 << logN) * sizeof(float2) : 0;
+}
+
+cudaError_t launch_range_compress_large(int logN, const DevJob *d_jobs, const RowItem *d_rows, int nrows,
+                                        int pairs, const float2 *tw1, const float2 *tw2, const float2 *twN,
+                                        float2 *work, int work_rows, cudaStream_t st) {
+    if (nrows <= 0) return cudaSuccess;
+    if (!tw1 || !tw2 || !twN || !work || work_rows < 1) return cudaErrorInvalidValue;
+    const int rb = work_rows;
+    switch (logN) {
+        case 15: return launch_four_step<7, 8>(logN, d_jobs, d_rows, nrows, pairs, tw1, tw2, twN, work, rb, st);
+        case 16: return launch_four_step<8, 8>(logN, d_jobs, d_rows, nrows, pairs, tw1, tw2, twN, work, rb, st);
+        case 17: return launch_four_step<8, 9>(logN, d_jobs, d_rows, nrows, pairs, tw1, tw2, twN, work, rb, st);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_range_compress(int logN, const DevJob *d_jobs, const RowItem *d_rows, int nrows, int pairs,

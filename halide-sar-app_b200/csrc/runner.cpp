@@ -65,7 +65,7 @@ int validate_job(const sarbp_job &j, int prec, int idx, bool rc_only, bool need_
     if ((long long)j.nu * j.nv > (1ll << 31)) return bad("image larger than 2^31 pixels");
     if (!is_pow2(j.n_fft) || j.n_fft < (1 << kMinLogN) || j.n_fft > (1 << kMaxLogN))
         return fail(SARBP_ERR_UNSUPPORTED, "job " + std::to_string(idx) +
-                                               ": N_fft must be a power of two in [16, 16384], got " +
+                                               ": N_fft must be a power of two in [16, 131072], got " +
                                                std::to_string(j.n_fft));
     if (j.taylor_s_l < 1) return bad("taylor must be >= 1");
     if (!(std::isfinite(j.delta_r))) return bad("delta_r must be finite");
@@ -226,6 +226,18 @@ cudaError_t DeviceInfo::twiddle(int logN, float2 **out) {
     *out = d;
     return cudaSuccess;
 }
+cudaError_t range_compress_rows(DeviceInfo *dev, int logN, const DevJob *d_jobs, const RowItem *d_rows, int nrows,
+                                int pairs, float2 *work, int work_rows, cudaStream_t st) {
+    float2 *tw = nullptr;
+    cudaError_t e = dev->twiddle(logN, &tw);
+    if (e != cudaSuccess) return e;
+    if (logN <= kMaxLogNSmem) return launch_range_compress(logN, d_jobs, d_rows, nrows, pairs, tw, st);
+    float2 *tw1 = nullptr, *tw2 = nullptr;
+    if ((e = dev->twiddle(logN / 2, &tw1)) != cudaSuccess) return e;
+    if ((e = dev->twiddle(logN - logN / 2, &tw2)) != cudaSuccess) return e;
+    return launch_range_compress_large(logN, d_jobs, d_rows, nrows, pairs, tw1, tw2, tw, work, work_rows, st);
+}
+
 cudaError_t DeviceInfo::record(int i, cudaStream_t st) {
     if (!timing) return cudaSuccess;
     if (!ev[i]) {
@@ -268,7 +280,9 @@ BpLaunch default_launch(const sarbp_opts *opts, int num_sms) {
 
 size_t Runner::job_scratch_bytes(const sarbp_job &j, const sarbp_opts *opts, bool resident_profiles) {
     const BpLaunch L = default_launch(opts, 148);
-    return layout_of(j, 0, L.tile_x, L.tile_y, false, j.precision == SARBP_PREC_NAIVE, resident_profiles).end;
+    const size_t work = resident_profiles ? 0 : align_up(rc_work_bytes(ilog2i(j.n_fft)), 256);
+    return layout_of(j, 0, L.tile_x, L.tile_y, false, j.precision == SARBP_PREC_NAIVE, resident_profiles).end +
+           work;
 }
 
 Runner::~Runner() {
@@ -330,6 +344,15 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
     for (int i = 0; i < njobs; ++i) {
         lay[i] = layout_of(jobs[i], off, L.tile_x, L.tile_y, rc_only, prec[i] == SARBP_PREC_NAIVE, resident(i));
         off = lay[i].end;
+    }
+    // work buffer of the four-step range compression (N_fft above
+    // 2^kMaxLogNSmem), shared by the batch's row groups one after another
+    size_t work_off = 0, work_bytes = 0;
+    for (int i = 0; i < njobs; ++i)
+        if (!resident(i)) work_bytes = std::max(work_bytes, rc_work_bytes(ilog2i(jobs[i].n_fft)));
+    if (work_bytes) {
+        work_off = off;
+        off = align_up(off + work_bytes, 256);
     }
     if (for_graph && (scratch_.cap < off || pool_ || status_pin_.cap < njobs * sizeof(JobScalars)))
         return fail(SARBP_ERR_STATE, "graph capture needs a prior run of the same jobs");
@@ -451,13 +474,18 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
     const WorkItem *d_items = reinterpret_cast<const WorkItem *>(d + o_items);
     int *d_cnt = reinterpret_cast<int *>(d + o_cnt);
 
-    // twiddle tables first (a one-time synchronous upload per N_fft)
+    // twiddle tables first (a one-time synchronous upload per N_fft; a
+    // four-step N_fft also needs the tables of its two sub-lengths)
     for (size_t g = 0; g < row_groups.size(); ++g) {
-        float2 *tw = nullptr;
-        if (for_graph && !dev_->has_twiddle(row_groups[g].first))
-            return fail(SARBP_ERR_STATE, "graph capture needs a prior run of the same jobs");
-        e = dev_->twiddle(row_groups[g].first, &tw);
-        if (e != cudaSuccess) return cuda_fail(e, "twiddle table");
+        const int l = row_groups[g].first;
+        const int need[3] = {l, l > kMaxLogNSmem ? l / 2 : l, l > kMaxLogNSmem ? l - l / 2 : l};
+        for (int n : need) {
+            float2 *tw = nullptr;
+            if (for_graph && !dev_->has_twiddle(n))
+                return fail(SARBP_ERR_STATE, "graph capture needs a prior run of the same jobs");
+            e = dev_->twiddle(n, &tw);
+            if (e != cudaSuccess) return cuda_fail(e, "twiddle table");
+        }
     }
     if (stage_events)
         for (int k = 0; k < DeviceInfo::kEvents; ++k) dev_->ev_recorded[k] = false;
@@ -503,10 +531,9 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         const int logN = row_groups[g].first;
         const size_t first = row_groups[g].second;
         const size_t count = rows[logN].size();
-        float2 *tw = nullptr;
-        e = dev_->twiddle(logN, &tw);
-        if (e != cudaSuccess) return cuda_fail(e, "twiddle table");
-        e = launch_range_compress(logN, d_jobs, d_rows + first, (int)count, rc_only ? 0 : 1, tw, rs);
+        float2 *work = work_bytes ? reinterpret_cast<float2 *>(sbase + work_off) : nullptr;
+        e = range_compress_rows(dev_, logN, d_jobs, d_rows + first, (int)count, rc_only ? 0 : 1, work,
+                                rc_work_rows(logN), rs);
         if (e != cudaSuccess) return cuda_fail(e, "range compression launch");
         dev_->launches++;
     }

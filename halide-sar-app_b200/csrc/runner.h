@@ -64,6 +64,12 @@ struct DeviceInfo {
     void release();
 };
 
+// Range compression of rows of one N_fft on st: the single-row kernel up to
+// 2^kMaxLogNSmem, above it the four-step FFT through `work`, which holds
+// work_rows rows of N_fft complex values (reused from launch to launch).
+cudaError_t range_compress_rows(DeviceInfo *dev, int logN, const DevJob *d_jobs, const RowItem *d_rows, int nrows,
+                                int pairs, float2 *work, int work_rows, cudaStream_t st);
+
 // Row slabs of a single job, for overlapping its host<->device copies with
 // compute: slab g covers tile rows [row0[g], row0[g + 1]).
 // After prep and range compression (on the main stream), slab g's tile

@@ -562,7 +562,7 @@ int sarbp_server_register(sarbp_server *s, const sarbp_job *host_aperture, long 
     if (rc) return rc;
     const size_t P = (size_t)h.npulses, S = (size_t)h.nsamples, N = (size_t)h.n_fft;
     // resident block [k32][k64][p32][p64][pairs]; set-up block
-    // [phs][scalars][descriptor][filt][wS][wP][pulse][rows]
+    // [phs][scalars][descriptor][filt][wS][wP][pulse][rows][four-step work]
     const size_t b_k32 = h.k_r ? a256(S * 4) : 0, b_k64 = h.k_r64 ? a256(S * 8) : 0;
     const size_t b_p32 = h.pos ? a256(P * 12) : 0, b_p64 = h.pos64 ? a256(P * 24) : 0;
     const size_t b_qp = a256(P * (N + 1) * sizeof(float4));
@@ -570,7 +570,10 @@ int sarbp_server_register(sarbp_server *s, const sarbp_job *host_aperture, long 
     const size_t o_sc = a256(P * S * 8), o_job = o_sc + a256(sizeof(JobScalars));
     const size_t o_filt = o_job + a256(sizeof(DevJob)), o_ws = o_filt + a256(S * 4), o_wp = o_ws + a256(S * 4);
     const size_t o_pulse = o_wp + a256(P * 4), o_rows = o_pulse + a256(P * sizeof(double4));
-    const size_t tmp_bytes = o_rows + a256(P * sizeof(RowItem));
+    int logN = 0;
+    while (((size_t)1 << logN) < N) ++logN;
+    const size_t o_work = o_rows + a256(P * sizeof(RowItem));
+    const size_t tmp_bytes = o_work + a256(rc_work_bytes(logN));
     {
         std::lock_guard<std::mutex> lk(s->mu);
         if (s->in_use + res_bytes + tmp_bytes > s->cap)
@@ -632,15 +635,15 @@ int sarbp_server_register(sarbp_server *s, const sarbp_job *host_aperture, long 
     dj.pulse = reinterpret_cast<double4 *>(tb + o_pulse);
     DevJob *d_job = reinterpret_cast<DevJob *>(tb + o_job);
     auto *rows = reinterpret_cast<RowItem *>(tb + o_rows);
-    float2 *tw = nullptr;
-    if (e == cudaSuccess) e = s->ctx->dev.twiddle(dj.logN, &tw);
     if (e == cudaSuccess) e = launch_store_job(dj, d_job, st);
     if (e == cudaSuccess) {
         launch_prep(d_job, 1, st);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = launch_fill_items(nullptr, 0, rows, (int)P, st);
-    if (e == cudaSuccess) e = launch_range_compress(dj.logN, d_job, rows, (int)P, 1, tw, st);
+    if (e == cudaSuccess)
+        e = range_compress_rows(&s->ctx->dev, dj.logN, d_job, rows, (int)P, 1, reinterpret_cast<float2 *>(tb + o_work),
+                                rc_work_rows(dj.logN), st);
     if (e == cudaSuccess) e = cudaFreeAsync(tmp, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {

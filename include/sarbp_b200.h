@@ -36,7 +36,7 @@ extern "C" {
 
 #define SARBP_OK 0
 #define SARBP_ERR_INVALID (-1)     /* bad argument, shape or size */
-#define SARBP_ERR_UNSUPPORTED (-2) /* e.g. N_fft not a power of two in [16, 16384] */
+#define SARBP_ERR_UNSUPPORTED (-2) /* e.g. N_fft not a power of two in [16, 131072] */
 #define SARBP_ERR_NOMEM (-3)       /* device or host allocation failed */
 #define SARBP_ERR_CUDA (-4)        /* a CUDA runtime call failed */
 #define SARBP_ERR_GEOMETRY (-5)    /* non-finite geometry, or a pixel tile whose

@@ -80,6 +80,8 @@ CASES = [
     ("odd_P_compat", dict(n=256, extent=25.0), 0, (100, 150, 219)),
     ("even_P_precise", dict(P=400, n=200, extent=20.0), 1, (64, 64, 64, 64, 64, 64, 16)),
     ("wide_tiles", dict(P=301, S=256, n=128, extent=80.0, R0=3000.0), 0, (120, 120, 61)),
+    # N_fft 32768: each chunk range-compressed by the four-step FFT
+    ("four_step_fft", dict(P=97, S=8192, df=1.5e6 * 424 / 8192, n=128, extent=20.0), 0, (40, 40, 17)),
 ]
 
 

@@ -49,11 +49,14 @@ def _job_for_rc(sb, torch, phs, k_r, taylor, N, pos):
 @pytest.mark.parametrize("P,S,N", [(469, 424, 1024), (470, 424, 1024), (33, 100, 16), (9, 7, 32),
                                    (65, 300, 512), (17, 1000, 2048), (1999, 1024, 4096),
                                    (5, 2048, 8192), (3, 4000, 16384), (12, 64, 128), (7, 120, 256),
-                                   (31, 33, 64)])
+                                   (31, 33, 64), (5, 8192, 32768), (4, 10000, 65536), (3, 6000, 131072),
+                                   (1100, 64, 32768), (3, 40000, 32768)])
 def test_range_compress_matches_oracle(sb, ctx, oracle, torch, P, S, N):
     """Fused window/filter/pad/shift + Stockham FFT + shift vs the f64
-    oracle for every radix schedule (N = 16 .. 16384), odd and even P, and
-    N < S (the centre of the pulse is kept)."""
+    oracle for every radix schedule (N = 16 .. 16384), the four-step FFT
+    above that (N = 32768 .. 131072; 1100 rows go through its work buffer in
+    two batches), odd and even P, and N < S (the centre of the pulse is
+    kept)."""
     rng = np.random.default_rng(P * 7 + S)
     phs = (rng.normal(size=(P, S)) + 1j * rng.normal(size=(P, S))).astype(np.complex64)
     k_r = rng.uniform(350, 400, size=S).astype(np.float32)
@@ -68,6 +71,47 @@ def test_range_compress_matches_oracle(sb, ctx, oracle, torch, P, S, N):
     # row by row too (rows of very different energy)
     for p in range(0, P, max(1, P // 7)):
         assert rel_l2(Q[p], ref[p]) < 5e-6
+
+
+@pytest.mark.parametrize("P,S,u", [(65, 8192, 2), (64, 3000, 6), (33, 12000, 6)])
+def test_four_step_fft_full_image(ctx, oracle, sb, P, S, u):
+    """N_fft above 16384 by the reference's rule (sarbp.cpp:258): S = 8192
+    at -u 2 (the reference's Sandia runs) and S >= 2731 at the default -u 6
+    give 32768 and more, range-compressed by the four-step FFT into the
+    interpolation pairs; whole 128^2 image against the reference-precision
+    oracle, compat tolerance."""
+    from sarbp_b200 import synth
+    d = synth.make("plain_small", seed=6,
+                   overrides=dict(P=P, S=S, df=1.5e6 * 424 / S, n=128, extent=20.0, upsample=u))
+    assert d["N_fft"] == sb.n_fft_for(S, u) and d["N_fft"] > 16384
+    pos32, k32 = d["pos"].astype(np.float32), d["k_r"].astype(np.float32)
+    img = ctx.backprojection_cuda(d["phs"], k32, d["taylor"], d["N_fft"], d["delta_r"], d["u"], d["v"],
+                                  pos32, d["r"])
+    ref = oracle.backprojection(d["phs"], k32, d["taylor"], d["N_fft"], d["delta_r"], pos32, d["r"],
+                                d["nu"], d["nv"], mode=oracle.MODE_REF)
+    e = rel_l2(img, ref)
+    print("N_fft %d (S %d, -u %d): rel-L2 %.3e" % (d["N_fft"], S, u, e))
+    assert e < REL_COMPAT
+    assert db_max_diff(img, ref, d["db"][0]) < DB_TOL
+
+
+def test_sandia_shape_sampled(ctx, oracle):
+    """The reference's Sandia GPU runs' range axis (8192 samples, -u 2 ->
+    N_fft 32768) on 2048 of its 8192 pulses and a 4096^2 image over 200 m:
+    whole image on the GPU, 2048 sampled pixels against the oracle."""
+    from sarbp_b200 import synth
+    d = synth.make("sandia_8192", seed=7, overrides=dict(P=2048, n=4096, extent=200.0))
+    assert d["N_fft"] == 32768
+    pos32, k32 = d["pos"].astype(np.float32), d["k_r"].astype(np.float32)
+    img = ctx.backprojection_cuda(d["phs"], k32, d["taylor"], d["N_fft"], d["delta_r"], d["u"], d["v"],
+                                  pos32, d["r"])
+    rng = np.random.default_rng(8)
+    idx = rng.choice(d["nu"] * d["nv"], 2048, replace=False)
+    ref = oracle.backproject(oracle.range_compress(d["phs"], k32, d["taylor"], d["N_fft"]), d["S"],
+                             d["delta_r"], k32, pos32, d["r"], d["nu"], d["nv"], out_idx=idx)
+    e = rel_l2(img.ravel()[idx], ref)
+    print("sandia shape (2048 pulses) sampled rel-L2 %.3e" % e)
+    assert e < REL_COMPAT
 
 
 def test_compat_plain_small_full_image(ctx, oracle, cfg1):
@@ -450,6 +494,9 @@ def test_errors_are_codes(sb, ctx, cfg1):
         d["u"], d["v"], kw.get("pos", pos32), d["r"])
     with pytest.raises(sb.SarbpError) as e:
         call(N=1000)
+    assert e.value.code == sb._lib.ERR_UNSUPPORTED
+    with pytest.raises(sb.SarbpError) as e:
+        call(N=1 << 18)  # above the four-step FFT's 131072
     assert e.value.code == sb._lib.ERR_UNSUPPORTED
     with pytest.raises(sb.SarbpError) as e:
         call(taylor=0)
