@@ -253,7 +253,7 @@ def run_reference(args, rank, world):
               "charged pro rata (%d of %d pixels)" % (n, P, P, n, nu * nv))
     out = {
         "impl": "reference",
-        "metric": "Gpixel*pulses/s (2048^2 x 1999 backprojection)",
+        "metric": metric_name(nu, nv, P),
         "value": value, "unit": "Gpixel*pulses/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_tot / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -433,7 +433,7 @@ def run_ours(args, rank, world, local_rank):
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     out = {
-        "metric": "Gpixel*pulses/s (2048^2 x 1999 backprojection)",
+        "metric": metric_name(nu, nv, P),
         "value": value, "unit": "Gpixel*pulses/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (split-precision; f64 per-pulse set-up)",
@@ -701,6 +701,13 @@ def run_batch(args, rank, world, local_rank):
     }
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def metric_name(nu, nv, P):
+    """The headline metric's name for an nu x nv image from P pulses
+    ("Gpixel*pulses/s (2048^2 x 1999 backprojection)" for plain_large)."""
+    img = "%d^2" % nu if nu == nv else "%dx%d" % (nu, nv)
+    return "Gpixel*pulses/s (%s x %d backprojection)" % (img, P)
 
 
 def per_job_measure(torch, ctx, stream, dev, njobs, seed, only, steps):

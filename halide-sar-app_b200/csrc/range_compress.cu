@@ -16,7 +16,11 @@
 // values per thread in registers, radix-16 passes (one leading radix-2/4/8
 // pass when log2 N is not a multiple of 4), rows exchanged through padded
 // shared memory between passes.  Twiddles come from a per-N table laid out
-// [r-1][j mod Ns] per pass so a warp's loads are contiguous.
+// [r-1][j mod Ns] per pass so a warp's loads are contiguous.  Up to
+// N = 2^kMaxLogNSmem one CTA holds a whole row; above it (the reference
+// sizes N_fft = 2^(floor(log2(S * upsample)) + 1), sarbp.cpp:258, so 8192
+// samples at -u 2 need 32768) the DFT is a four-step FFT of two such
+// sub-DFTs through a work buffer (see rc_cols_kernel / rc_rows_kernel).
 #include "internal.h"
 #include "kernels.h"
 
