@@ -391,7 +391,8 @@ int sarbp_autotune(sarbp_ctx *ctx, const sarbp_job *jobs, int njobs,
  * forms each image.  Runs the same kernels as sarbp_backprojection_device on
  * `cuda_stream`, with all scratch in one static 64 MiB device array of the
  * library:
- *  - jobs needing more scratch than that return SARBP_ERR_UNSUPPORTED
+ *  - jobs needing more scratch than that, or an N_fft above 16384, return
+ *    SARBP_ERR_UNSUPPORTED
  *    (roughly: 256 KiB of twiddle tables + 16 B x npulses x n_fft + 32 B x
  *    npulses x tiles of 32x32 pixels + 8 B x pixels);
  *  - every call shares the array and it keeps the last call's contents, so
