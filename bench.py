@@ -72,6 +72,9 @@ def parse():
                     help="batch96: time every job alone instead (per-job rates by tile regime)")
     ap.add_argument("--only-job", type=int, default=-1,
                     help="batch96: run job J alone --steps times and exit (profiling one job)")
+    ap.add_argument("--set", action="append", default=[], metavar="KEY=VALUE",
+                    help="override a field of the synthetic config (e.g. P=1024 n=2048; profiling "
+                         "captures of a smaller case of the same kernels)")
     ap.add_argument("--serve-rates", default="20,50,100,200,400", help="serve: arrival rates (req/s)")
     ap.add_argument("--serve-requests", type=int, default=2000, help="serve: requests per rate")
     ap.add_argument("--serve-lanes", type=int, default=3, help="serve: concurrent batches")
@@ -276,7 +279,8 @@ def config_block(data, world):
             "image": [data["nu"], data["nv"]], "npulses": data["P"], "nsamples": data["S"],
             "n_fft": data["N_fft"], "taylor": data["taylor"], "precision": "compat",
             "parallelism": "replicas%d" % world,
-            "l2": "inputs+outputs ~250 MB per step (> 126 MB L2), no flush"}
+            "l2": "inputs+outputs %.0f MB per step (> 126 MB L2), no flush" % (
+                (8.0 * data["P"] * data["S"] + 40.0 * data["nu"] * data["nv"]) / 1e6)}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -287,7 +291,11 @@ def run_ours(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    data = synth.make(args.config, seed=2 + rank)
+    over = {}
+    for kv in args.set:
+        k, v = kv.split("=", 1)
+        over[k] = float(v) if "." in v or "e" in v else int(v)
+    data = synth.make(args.config, seed=2 + rank, overrides=over or None)
     nu, nv, P, S = data["nu"], data["nv"], data["P"], data["S"]
     units = float(nu) * nv * P
 
