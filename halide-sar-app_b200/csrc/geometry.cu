@@ -111,6 +111,34 @@ __device__ __forceinline__ bool make_record(const DevJob &jb, const TileInfo &t,
 
 
 
+// Half-width K (bins) of the range window every pulse's bins of this tile
+// fall in: K = ceil(1.004 X / lsr) + 2 for a bound X on |Delta| =
+// |R - |pos - r|| over the tile's pixels r = rc + d and all pulses.  The
+// triangle inequality gives X = rho.  Tighter, with s = w_hat . d:
+//   |Delta| = |2 R s - |d|^2| / (R + |pos - r|) <= (2 R |s| + rho^2) / (2 R - rho),
+//   |s| <= sum_i h_i |w_hat_i|   (d inside the bounding box of half-extents h),
+//   |w_hat_i| <= los_abs_i + 2 |rc| / pos_min,
+// since w_hat = (pos - rc) / |pos - rc| differs from pos / |pos| by at most
+// 2 |rc| / |pos|, with R >= pos_min - |rc|.  For an image plane seen from
+// above at an angle this halves the window (more pulses per staged chunk).
+__device__ __forceinline__ int window_half_width(const DevJob &jb, float rho_f, const double (&rc)[3],
+                                                 const double (&hh)[3]) {
+    const double rho = (double)rho_f;
+    double X = rho;
+    const double pmin = jb.sc->pos_min;
+    const double c = sqrt(rc[0] * rc[0] + rc[1] * rc[1] + rc[2] * rc[2]);
+    if (pmin > 0.0 && isfinite(pmin) && 2.0 * c < pmin) {
+        const double Rt = pmin - c, dl = 2.0 * c / pmin;
+        if (Rt > 2.0 * rho) {
+            double B = 0.0;
+            for (int i = 0; i < 3; ++i) B += hh[i] * fmin(1.0, jb.sc->los_abs[i] + dl);
+            B *= 1.0 + 1e-9;
+            X = fmin(rho, (2.0 * Rt * B + rho * rho) / (2.0 * Rt - rho));
+        }
+    }
+    return (int)ceil(X * jb.inv_lsr * 1.004) + 2;
+}
+
 __device__ __forceinline__ double warp_min_d(double v) {
     for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
@@ -176,7 +204,7 @@ __global__ void __launch_bounds__(kThreadsGeom, GP <= 4 ? 4 : 2)
             sbox[warp][3 + d] = mx[d];
         }
     __syncthreads();
-    double rc[3], hd2 = 0.0;
+    double rc[3], hd2 = 0.0, hh[3];
     for (int d = 0; d < 3; ++d) {
         double a = sbox[0][d], b = sbox[0][3 + d];
         for (int w = 1; w < kWarps; ++w) {
@@ -184,6 +212,7 @@ __global__ void __launch_bounds__(kThreadsGeom, GP <= 4 ? 4 : 2)
             b = fmax(b, sbox[w][3 + d]);
         }
         rc[d] = a <= b ? 0.5 * (a + b) : 0.0;
+        hh[d] = a <= b ? 0.5 * (b - a) : 0.0;
         if (a <= b) hd2 += 0.25 * (b - a) * (b - a);
     }
     const double k_c = jb.sc->k_c;
@@ -253,7 +282,7 @@ __global__ void __launch_bounds__(kThreadsGeom, GP <= 4 ? 4 : 2)
         t.rc[1] = rc[1];
         t.rc[2] = rc[2];
         t.rho = rho * (1.0f + 1e-5f) + 1e-6f;
-        t.K = (int)ceilf(t.rho * (float)jb.inv_lsr * 1.004f) + 2;
+        t.K = window_half_width(jb, t.rho, rc, hh);
         t.planar = planar;
         t.wide = wide ? 1 : 0;
         t.w0[0] = w0f[0];

@@ -29,6 +29,11 @@ struct JobScalars {
     double k_c;                 // k_r[S/2] by precision mode (prep kernel)
     int status;                 // kStatus* bits
     int pad[3];
+    // over the job's pulses (prep kernel, f64 from the antenna positions):
+    // max |pos_i| / |pos| per axis and min |pos|, which bound the tiles'
+    // line-of-sight components and so their range windows
+    double los_abs[3];
+    double pos_min;
 };
 
 // Tiles wider than this many radians of k_c * (half-diagonal) are "wide":

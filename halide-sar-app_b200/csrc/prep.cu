@@ -70,6 +70,7 @@ __global__ void __launch_bounds__(kPrepThreads) prep_kernel(const DevJob *__rest
             }
         }
     } else {
+        double la[3] = {0.0, 0.0, 0.0}, nmin = INFINITY;
         for (int p = threadIdx.x; p < jb.P; p += blockDim.x) {
             double4 g;
             if (jb.precision == SARBP_PREC_PRECISE_) {
@@ -94,6 +95,21 @@ __global__ void __launch_bounds__(kPrepThreads) prep_kernel(const DevJob *__rest
                 g = make_double4(x, y, z, (double)__fsqrt_rn(s));
             }
             jb.pulse[p] = g;
+            const double n = sqrt(g.x * g.x + g.y * g.y + g.z * g.z);
+            if (n > 0.0 && isfinite(n)) {
+                la[0] = fmax(la[0], fabs(g.x) / n);
+                la[1] = fmax(la[1], fabs(g.y) / n);
+                la[2] = fmax(la[2], fabs(g.z) / n);
+                nmin = fmin(nmin, n);
+            } else {
+                nmin = 0.0;  // no bound from this job's positions
+            }
+        }
+        for (int i = 0; i < 3; ++i) la[i] = block_max(la[i], sred);
+        nmin = -block_max(-nmin, sred);
+        if (threadIdx.x == 0) {
+            for (int i = 0; i < 3; ++i) jb.sc->los_abs[i] = la[i];
+            jb.sc->pos_min = nmin;
         }
     }
 }
