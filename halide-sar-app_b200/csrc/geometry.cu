@@ -3,10 +3,11 @@
 // tile_setup_kernel (one CTA per (job, tile)) forms the tile's geometry and
 // then its pulse records:
 //   rc    = centre of the bounding box of the tile's pixel positions
-//   wide  = k_c * (bounding-box half-diagonal) > kWideRad; then w0 = unit
+//   wide  = k_c * rho > kWideRad (rho below); then w0 = unit
 //           vector from rc to the mid-aperture antenna
 //   rho   = max |(f32)(r - rc)|, the same f32 offsets the backprojection
-//           kernel forms, padded; K = ceil(1.004 rho / lsr) + 2
+//           kernel forms, padded; K = ceil(1.004 X / lsr) + 2 for a bound X
+//           <= rho on the pixels' range offsets (window_half_width)
 //   fin   = exp(+j k_c dr(pixel, P/2)) per pixel (backprojection.cpp:135),
 //           dr = |pos| - |r - pos| in f64, phase reduced in f64; wide tiles
 //           multiply in exp(-j w0 . k_c (r - rc)), also in f64
@@ -114,15 +115,18 @@ __device__ __forceinline__ bool make_record(const DevJob &jb, const TileInfo &t,
 // Half-width K (bins) of the range window every pulse's bins of this tile
 // fall in: K = ceil(1.004 X / lsr) + 2 for a bound X on |Delta| =
 // |R - |pos - r|| over the tile's pixels r = rc + d and all pulses.  The
-// triangle inequality gives X = rho.  Tighter, with s = w_hat . d:
+// triangle inequality gives X = rho.  Tighter, with s = w_hat . d and E the
+// job's orthonormal image-plane frame (prep kernel):
 //   |Delta| = |2 R s - |d|^2| / (R + |pos - r|) <= (2 R |s| + rho^2) / (2 R - rho),
-//   |s| <= sum_i h_i |w_hat_i|   (d inside the bounding box of half-extents h),
-//   |w_hat_i| <= los_abs_i + 2 |rc| / pos_min,
+//   |s| <= sum_i |d . E_i| |w_hat . E_i|,  |d . E_i| <= hq_i over the tile,
+//   |w_hat . E_i| <= los_abs_i + 2 |rc| / pos_min,
 // since w_hat = (pos - rc) / |pos - rc| differs from pos / |pos| by at most
-// 2 |rc| / |pos|, with R >= pos_min - |rc|.  For an image plane seen from
-// above at an angle this halves the window (more pulses per staged chunk).
+// 2 |rc| / |pos|, with R >= pos_min - |rc|.  hq comes from f32 offsets and
+// an f32 copy of E, so it is taken with margins well above their rounding.
+// For an image plane seen from above at an angle this halves the window
+// (more pulses per staged chunk), whatever the plane's orientation.
 __device__ __forceinline__ int window_half_width(const DevJob &jb, float rho_f, const double (&rc)[3],
-                                                 const double (&hh)[3]) {
+                                                 const float (&hq)[3]) {
     const double rho = (double)rho_f;
     double X = rho;
     const double pmin = jb.sc->pos_min;
@@ -131,8 +135,9 @@ __device__ __forceinline__ int window_half_width(const DevJob &jb, float rho_f, 
         const double Rt = pmin - c, dl = 2.0 * c / pmin;
         if (Rt > 2.0 * rho) {
             double B = 0.0;
-            for (int i = 0; i < 3; ++i) B += hh[i] * fmin(1.0, jb.sc->los_abs[i] + dl);
-            B *= 1.0 + 1e-9;
+            for (int i = 0; i < 3; ++i)
+                B += ((double)hq[i] * (1.0 + 1e-5) + 1e-6 * rho) * fmin(1.0, jb.sc->los_abs[i] + dl + 1e-9);
+            B = B * (1.0 + 1e-6) + 1e-5 * rho;
             X = fmin(rho, (2.0 * Rt * B + rho * rho) / (2.0 * Rt - rho));
         }
     }
@@ -159,6 +164,7 @@ __global__ void __launch_bounds__(kThreadsGeom, GP <= 4 ? 4 : 2)
     __shared__ double sbox[kWarps][6];
     __shared__ float srho[kWarps];
     __shared__ int sflags[kWarps][2];
+    __shared__ float shq[kWarps][3];
     __shared__ TileInfo s_tile;
     const WorkItem wi = items[blockIdx.x];
     const DevJob &jb = jobs[wi.job];
@@ -204,7 +210,7 @@ __global__ void __launch_bounds__(kThreadsGeom, GP <= 4 ? 4 : 2)
             sbox[warp][3 + d] = mx[d];
         }
     __syncthreads();
-    double rc[3], hd2 = 0.0, hh[3];
+    double rc[3];
     for (int d = 0; d < 3; ++d) {
         double a = sbox[0][d], b = sbox[0][3 + d];
         for (int w = 1; w < kWarps; ++w) {
@@ -212,27 +218,59 @@ __global__ void __launch_bounds__(kThreadsGeom, GP <= 4 ? 4 : 2)
             b = fmax(b, sbox[w][3 + d]);
         }
         rc[d] = a <= b ? 0.5 * (a + b) : 0.0;
-        hh[d] = a <= b ? 0.5 * (b - a) : 0.0;
-        if (a <= b) hd2 += 0.25 * (b - a) * (b - a);
+    }
+    // radius, extents in the job's image-plane frame and flags of the tile,
+    // from the same f32 offsets the backprojection kernel forms
+    float Ef[3][3];  // the job's image-plane frame (f32 copy)
+    for (int i = 0; i < 3; ++i)
+        for (int c = 0; c < 3; ++c) Ef[i][c] = (float)jb.sc->frame[i][c];
+    float hq[3] = {0.f, 0.f, 0.f};  // max |(r - rc) . E_i| over the tile's pixels
+    float rho = 0.0f;
+    int planar = 1;
+#pragma unroll
+    for (int k = 0; k < GP; ++k) {
+        if (!(live & (1u << k))) continue;
+        const float ox = (float)(px[k] - rc[0]), oy = (float)(py[k] - rc[1]), oz = (float)(pz[k] - rc[2]);
+        rho = fmaxf(rho, sqrtf(fmaf(ox, ox, fmaf(oy, oy, oz * oz))));
+        planar &= (oz == 0.0f);
+        for (int i = 0; i < 3; ++i) hq[i] = fmaxf(hq[i], fabsf(fmaf(ox, Ef[i][0], fmaf(oy, Ef[i][1], oz * Ef[i][2]))));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        rho = fmaxf(rho, __shfl_xor_sync(0xffffffffu, rho, o));
+        planar &= __shfl_xor_sync(0xffffffffu, planar, o);
+        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+        for (int i = 0; i < 3; ++i) hq[i] = fmaxf(hq[i], __shfl_xor_sync(0xffffffffu, hq[i], o));
+    }
+    if (lane == 0) {
+        srho[warp] = rho;
+        sflags[warp][0] = planar;
+        sflags[warp][1] = bad;
+        for (int i = 0; i < 3; ++i) shq[warp][i] = hq[i];
+    }
+    __syncthreads();
+    for (int w = 0; w < kWarps; ++w) {
+        rho = fmaxf(rho, srho[w]);
+        planar &= sflags[w][0];
+        bad |= sflags[w][1];
+        for (int i = 0; i < 3; ++i) hq[i] = fmaxf(hq[i], shq[w][i]);
     }
     const double k_c = jb.sc->k_c;
     const double4 pm = jb.pulse[jb.P / 2];
-    // wide tile: reference direction w0 toward the mid-aperture antenna; the
-    // phase w0 . k_c (r - rc) leaves the pulse loop and enters fin in f64
+    // wide tile (k_c times the tile's radius above kWideRad): reference
+    // direction w0 toward the mid-aperture antenna; the phase w0 . k_c (r - rc)
+    // leaves the pulse loop and enters fin in f64
     float w0f[3] = {0.f, 0.f, 0.f};
     bool wide = false;
     {
         const double gx = pm.x - rc[0], gy = pm.y - rc[1], gz = pm.z - rc[2];
         const double g = sqrt(gx * gx + gy * gy + gz * gz);
-        if (k_c * sqrt(hd2) > kWideRad && g > 0.0 && isfinite(g)) {
+        if (k_c * (double)rho > kWideRad && g > 0.0 && isfinite(g)) {
             wide = true;
             w0f[0] = (float)(gx / g);
             w0f[1] = (float)(gy / g);
             w0f[2] = (float)(gz / g);
         }
     }
-    float rho = 0.0f;
-    int planar = 1;
 #pragma unroll
     for (int k = 0; k < GP; ++k) {
         const int idx = threadIdx.x + k * kThreadsGeom;
@@ -242,9 +280,6 @@ __global__ void __launch_bounds__(kThreadsGeom, GP <= 4 ? 4 : 2)
         const double x = px[k], y = py[k], z = pz[k];
         float2 f = make_float2(0.f, 0.f);
         if (live & (1u << k)) {
-            const float ox = (float)(x - rc[0]), oy = (float)(y - rc[1]), oz = (float)(z - rc[2]);
-            rho = fmaxf(rho, sqrtf(fmaf(ox, ox, fmaf(oy, oy, oz * oz))));
-            planar &= (oz == 0.0f);
             const double ex = x - pm.x, ey = y - pm.y, ez = z - pm.z;
             const double drm = pm.w - sqrt(ex * ex + ey * ey + ez * ez);
             double th = drm * (k_c * kInv2Pi);
@@ -260,29 +295,13 @@ __global__ void __launch_bounds__(kThreadsGeom, GP <= 4 ? 4 : 2)
         }
         jb.fin[(long long)iy * jb.nu + ix] = f;
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        rho = fmaxf(rho, __shfl_xor_sync(0xffffffffu, rho, o));
-        planar &= __shfl_xor_sync(0xffffffffu, planar, o);
-        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
-    }
-    if (lane == 0) {
-        srho[warp] = rho;
-        sflags[warp][0] = planar;
-        sflags[warp][1] = bad;
-    }
-    __syncthreads();
     if (threadIdx.x == 0) {
-        for (int w = 1; w < kWarps; ++w) {
-            rho = fmaxf(rho, srho[w]);
-            planar &= sflags[w][0];
-            bad |= sflags[w][1];
-        }
         TileInfo t;
         t.rc[0] = rc[0];
         t.rc[1] = rc[1];
         t.rc[2] = rc[2];
         t.rho = rho * (1.0f + 1e-5f) + 1e-6f;
-        t.K = window_half_width(jb, t.rho, rc, hh);
+        t.K = window_half_width(jb, t.rho, rc, hq);
         t.planar = planar;
         t.wide = wide ? 1 : 0;
         t.w0[0] = w0f[0];

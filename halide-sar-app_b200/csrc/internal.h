@@ -29,9 +29,11 @@ struct JobScalars {
     double k_c;                 // k_r[S/2] by precision mode (prep kernel)
     int status;                 // kStatus* bits
     int pad[3];
-    // over the job's pulses (prep kernel, f64 from the antenna positions):
-    // max |pos_i| / |pos| per axis and min |pos|, which bound the tiles'
-    // line-of-sight components and so their range windows
+    // prep kernel, f64: an orthonormal frame E of the job's image plane
+    // (rows; the grid axes, or the first pixels of r), and over the job's
+    // antenna positions max |pos . E_i| / |pos| and min |pos|, which bound
+    // the tiles' line-of-sight components and so their range windows
+    double frame[3][3];
     double los_abs[3];
     double pos_min;
 };

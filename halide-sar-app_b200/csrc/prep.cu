@@ -40,6 +40,35 @@ __device__ double taylor_w(const DevJob &jb, int num, int x) {
     return w;
 }
 
+// An orthonormal frame (rows of E) for the tiles' window bound: the image
+// plane the reference builds by default, u_hat along the ground projection
+// of the mid-aperture position, v_hat = z x u_hat, n_hat = z
+// (img_plane.cpp:56-75 with n_hat = (0, 0, 1)); the x, y, z axes when that
+// projection vanishes.  It depends on the antenna positions only, so the
+// r-array and axes forms of a job get the same frame.  Any orthonormal frame
+// keeps the bound valid; the image plane's own makes it tight.
+__device__ void image_frame(const DevJob &jb, double (&E)[3][3]) {
+    for (int i = 0; i < 3; ++i)
+        for (int c = 0; c < 3; ++c) E[i][c] = i == c ? 1.0 : 0.0;
+    const int m = jb.P / 2;
+    double x, y;
+    if (jb.precision == SARBP_PREC_PRECISE_ && jb.pos64) {
+        x = jb.pos64[3 * m];
+        y = jb.pos64[3 * m + 1];
+    } else {
+        x = jb.pos32[3 * m];
+        y = jb.pos32[3 * m + 1];
+    }
+    const double n = sqrt(x * x + y * y);
+    if (!(n > 0.0) || !isfinite(n)) return;
+    E[0][0] = x / n;
+    E[0][1] = y / n;
+    E[0][2] = 0.0;
+    E[1][0] = -y / n;
+    E[1][1] = x / n;
+    E[1][2] = 0.0;
+}
+
 __global__ void __launch_bounds__(kPrepThreads) prep_kernel(const DevJob *__restrict__ jobs) {
     __shared__ double sred[32];
     const DevJob &jb = jobs[blockIdx.x];
@@ -70,6 +99,8 @@ __global__ void __launch_bounds__(kPrepThreads) prep_kernel(const DevJob *__rest
             }
         }
     } else {
+        double E[3][3];
+        image_frame(jb, E);
         double la[3] = {0.0, 0.0, 0.0}, nmin = INFINITY;
         for (int p = threadIdx.x; p < jb.P; p += blockDim.x) {
             double4 g;
@@ -97,9 +128,8 @@ __global__ void __launch_bounds__(kPrepThreads) prep_kernel(const DevJob *__rest
             jb.pulse[p] = g;
             const double n = sqrt(g.x * g.x + g.y * g.y + g.z * g.z);
             if (n > 0.0 && isfinite(n)) {
-                la[0] = fmax(la[0], fabs(g.x) / n);
-                la[1] = fmax(la[1], fabs(g.y) / n);
-                la[2] = fmax(la[2], fabs(g.z) / n);
+                for (int i = 0; i < 3; ++i)
+                    la[i] = fmax(la[i], fabs(g.x * E[i][0] + g.y * E[i][1] + g.z * E[i][2]) / n);
                 nmin = fmin(nmin, n);
             } else {
                 nmin = 0.0;  // no bound from this job's positions
@@ -108,7 +138,10 @@ __global__ void __launch_bounds__(kPrepThreads) prep_kernel(const DevJob *__rest
         for (int i = 0; i < 3; ++i) la[i] = block_max(la[i], sred);
         nmin = -block_max(-nmin, sred);
         if (threadIdx.x == 0) {
-            for (int i = 0; i < 3; ++i) jb.sc->los_abs[i] = la[i];
+            for (int i = 0; i < 3; ++i) {
+                jb.sc->los_abs[i] = la[i];
+                for (int c = 0; c < 3; ++c) jb.sc->frame[i][c] = E[i][c];
+            }
             jb.sc->pos_min = nmin;
         }
     }

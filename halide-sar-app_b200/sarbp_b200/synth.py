@@ -109,6 +109,14 @@ def make(name="plain_small", seed=1, with_r=True, overrides=None, nthreads=0):
     scat = scene(cfg["nscat"], cfg["half"], cfg["clutter"], seed)
     phs, pos, k_r = phase_history(cfg["S"], cfg["P"], cfg["f0"], cfg["df"], cfg["R0"], cfg["dep"],
                                   cfg["span"], scat, cfg["snr"], seed, nthreads)
+    if cfg.get("az"):
+        # the whole geometry turned by az degrees about z (the phase history
+        # only sees relative positions): the image plane's axes turn with it
+        a = np.deg2rad(cfg["az"])
+        rot = np.array([[np.cos(a), -np.sin(a), 0.0], [np.sin(a), np.cos(a), 0.0], [0.0, 0.0, 1.0]])
+        pos = pos @ rot.T
+        scat = scat.copy()
+        scat[:, :3] = scat[:, :3] @ rot.T
     delta_r = C / (2.0 * cfg["S"] * cfg["df"])
     g = grid_plane(cfg["n"], cfg["extent"], pos, delta_r, cfg["S"], cfg["P"])
     out = dict(cfg=cfg, name=name, phs=phs, pos=pos, k_r=k_r, delta_r=delta_r,

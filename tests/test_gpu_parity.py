@@ -131,18 +131,21 @@ def test_compat_plain_small_full_image(ctx, oracle, cfg1):
     assert dbd < DB_TOL
 
 
-@pytest.mark.parametrize("R0,extent,n", [
-    (400.0, 120.0, 256),    # near field: closed form (series order 3), wide tiles
-    (2000.0, 80.0, 256),    # four-term series, wide tiles
-    (10e3, 150.0, 256),     # far, coarse pixels (0.59 m): wide tiles, low orders
-    (10e3, 20.0, 256),      # far, fine pixels: narrow tiles, two-term series
+@pytest.mark.parametrize("R0,extent,n,u,az", [
+    (400.0, 120.0, 256, 2, 0.0),    # near field: closed form (series order 3), wide tiles
+    (2000.0, 80.0, 256, 2, 0.0),    # four-term series, wide tiles
+    (10e3, 150.0, 256, 2, 0.0),     # far, coarse pixels (0.59 m): wide tiles, low orders
+    (10e3, 20.0, 256, 2, 0.0),      # far, fine pixels: narrow tiles, two-term series
+    (10e3, 60.0, 256, 6, 35.0),     # -u 6, pixels at the range resolution, plane turned 35 deg
+    (3000.0, 60.0, 256, 6, -60.0),  # the same nearer, turned the other way
 ])
-def test_geometry_regimes(ctx, oracle, R0, extent, n):
-    """Standoff and pixel size across the kernel's regimes (which series
-    order a pulse needs, and whether a tile is wide) against the
-    reference-precision oracle, whole image, compat tolerance."""
+def test_geometry_regimes(ctx, oracle, R0, extent, n, u, az):
+    """Standoff, pixel size, upsampling and image-plane orientation across
+    the kernel's regimes (which series order a pulse needs, whether a tile is
+    wide, how narrow a window the tile's line-of-sight extent allows)
+    against the reference-precision oracle, whole image, compat tolerance."""
     from sarbp_b200 import synth
-    d = synth.make("plain_small", seed=3, overrides=dict(R0=R0, extent=extent, n=n))
+    d = synth.make("plain_small", seed=3, overrides=dict(R0=R0, extent=extent, n=n, upsample=u, az=az))
     pos32 = d["pos"].astype(np.float32)
     k32 = d["k_r"].astype(np.float32)
     img = ctx.backprojection_cuda(d["phs"], k32, d["taylor"], d["N_fft"], d["delta_r"], d["u"], d["v"],
@@ -151,7 +154,7 @@ def test_geometry_regimes(ctx, oracle, R0, extent, n):
                                 d["nu"], d["nv"], mode=oracle.MODE_REF)
     e = rel_l2(img, ref)
     dbd = db_max_diff(img, ref, d["db"][0])
-    print("R0 %.0f m, pixel %.3f m: rel-L2 %.3e  dB max diff %.4f" % (R0, extent / n, e, dbd))
+    print("R0 %.0f m, pixel %.3f m, -u %d, az %.0f: rel-L2 %.3e  dB max diff %.4f" % (R0, extent / n, u, az, e, dbd))
     assert e < REL_COMPAT
     assert dbd < DB_TOL
 
