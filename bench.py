@@ -44,7 +44,7 @@ SERVE_RATES = (100.0, 200.0, 400.0)  # req/s of the serving block of the default
 SERVE_REQUESTS = 400                 # requests per rate there
 # DRAM bytes (read + write) of one bp_tile_kernel launch, from an ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum) of the default plain_large step
-NCU_BP_TRAFFIC = {"plain_large": 571.163392e6 + 82.052096e6}
+NCU_BP_TRAFFIC = {"plain_large": 565.913856e6 + 83.077632e6}
 
 
 def parse():
