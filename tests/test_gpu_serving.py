@@ -161,6 +161,30 @@ def test_registered_aperture_skips_upload_and_range_compression(ctx, sb, pool):
         srv.close()
 
 
+def test_registered_aperture_with_four_step_fft(ctx, sb):
+    """An aperture whose N_fft (32768: 8192 samples at -u 2) takes the
+    four-step range compression, registered once: its requests give the
+    same image bit for bit as a request that brings the phase history."""
+    from sarbp_b200 import synth
+    from sarbp_b200.batch import HostJob
+    cfg = dict(synth.batch_jobs(njobs=1, seed=31)[0], P=120, S=8192, df=1.5e6 * 424 / 8192, n=128,
+               extent=20.0, upsample=2, taylor=20, taylor_mode=0)
+    hj = HostJob(cfg)
+    assert hj.data["N_fft"] == 32768
+    srv = sb.Server(ctx, hbm_cap_bytes=8e9, lanes=2, max_batch=4, precision=sb.PREC_PRECISE)
+    try:
+        rid, direct = _submit(srv, hj, sb.PREC_PRECISE)
+        assert srv.wait(rid, 60.0) == 0
+        ap = srv.register(hj.job(hj.new_outputs()[0], precision=sb.PREC_PRECISE))
+        out = hj.new_outputs()[0]
+        r = srv.submit_on(ap, hj.job(out), keep=out)
+        assert srv.wait(r, 60.0) == 0
+        assert np.array_equal(out, direct) and np.all(np.isfinite(out))
+        srv.unregister(ap)
+    finally:
+        srv.close()
+
+
 def test_register_over_budget_is_an_admission_error(ctx, sb):
     from sarbp_b200 import _lib, synth
     from sarbp_b200.batch import HostJob

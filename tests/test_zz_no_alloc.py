@@ -129,3 +129,6 @@ def test_noalloc_rejects_jobs_larger_than_its_scratch(sb):
     rc = L.sarbp_backprojection_noalloc(ctypes.byref(job), None, None)
     assert rc == _lib.ERR_UNSUPPORTED
     assert b"MiB" in L.sarbp_last_error()
+    # N_fft above 16384 (the four-step FFT's work buffer) is not taken either
+    job = sb.make_job(64, 8, 32768, 17, 32, 32, 0.25, 16, 16, 16, 16, r=16)
+    assert L.sarbp_backprojection_noalloc(ctypes.byref(job), None, None) == _lib.ERR_UNSUPPORTED
