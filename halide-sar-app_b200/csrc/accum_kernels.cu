@@ -13,6 +13,8 @@
 // and once at the end
 //   finalize_kernel      out[nv-1-y][x] = acc[y][x] * fin[y][x]
 //                        (backprojection.cpp:130-135), max |z| for dB/u8.
+// The combine kernel does the same for one-shot jobs formed in pulse parts
+// (each part's sums in its own slice; see DevJob::nsplit).
 #include <cstdint>
 
 #include "internal.h"
@@ -60,9 +62,43 @@ __global__ void __launch_bounds__(kThreads) finalize_kernel(const DevJob *__rest
     }
 }
 
+// Jobs formed in pulse parts: out[nv-1-y][x] = (sum of the nsplit slices,
+// in slice order) * fin[y][x], the same arithmetic as the backprojection
+// kernel's epilogue; max |z| for dB/u8.  blockIdx.y: entry of the job list.
+__global__ void __launch_bounds__(kThreads) combine_parts_kernel(const DevJob *__restrict__ jobs,
+                                                                 const int *__restrict__ list) {
+    const DevJob &jb = jobs[list[blockIdx.y]];
+    const long long n = (long long)jb.nu * jb.nv;
+    const int ns = jb.nsplit;
+    double zmax = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int iy = (int)(i / jb.nu), ix = (int)(i - (long long)iy * jb.nu);
+        float2 a = jb.parts[i];
+        for (int k = 1; k < ns; ++k) {
+            const float2 b = jb.parts[(long long)k * n + i];
+            a.x += b.x;
+            a.y += b.y;
+        }
+        const float2 f = jb.fin[i];
+        const double zr = (double)fmaf(a.x, f.x, -a.y * f.y);
+        const double zi = (double)fmaf(a.x, f.y, a.y * f.x);
+        jb.out[(long long)(jb.nv - 1 - iy) * jb.nu + ix] = make_double2(zr, zi);
+        zmax = fmax(zmax, sqrt(zr * zr + zi * zi));
+    }
+    for (int o = 16; o > 0; o >>= 1) zmax = fmax(zmax, __shfl_xor_sync(0xffffffffu, zmax, o));
+    __shared__ double s[kThreads / 32];
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = zmax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kThreads / 32; ++w) zmax = fmax(zmax, s[w]);
+        atomicMax(&jb.sc->maxabs, (unsigned long long)__double_as_longlong(zmax));
+    }
+}
+
 __global__ void fill_items_kernel(WorkItem *items, int ntiles, RowItem *rows, int nrows) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < ntiles) items[t] = WorkItem{0, t};
+    if (t < ntiles) items[t] = WorkItem{0, t, 0};
     if (t < nrows) rows[t] = RowItem{0, t};
 }
 
@@ -88,6 +124,16 @@ cudaError_t launch_finalize(const DevJob *d_job, long long npix, int num_sms, cu
     long long b = (npix + kThreads - 1) / kThreads;
     if (b > (long long)num_sms * 8) b = (long long)num_sms * 8;
     finalize_kernel<<<(int)(b < 1 ? 1 : b), kThreads, 0, st>>>(d_job);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_combine_parts(const DevJob *d_jobs, const int *d_list, int nlist, long long max_pixels,
+                                 int num_sms, cudaStream_t st) {
+    if (nlist <= 0) return cudaSuccess;
+    long long b = (max_pixels + kThreads - 1) / kThreads;
+    const long long cap = ((long long)num_sms * 8 + nlist - 1) / nlist;
+    if (b > cap) b = cap;
+    combine_parts_kernel<<<dim3((unsigned)(b < 1 ? 1 : b), (unsigned)nlist), kThreads, 0, st>>>(d_jobs, d_list);
     return cudaGetLastError();
 }
 

@@ -45,13 +45,15 @@ struct PlaneAxes {
 // the phase history and a few position rows are up, the second twice that,
 // the last as small as the first so that little of the image is still to
 // come down when the kernels end; the rest in equal slabs of at least 8
-// tile rows, at most kMaxSlabs slabs in all.
+// tile rows, at most kMaxSlabs slabs in all.  None when the caller asked for
+// pulse parts (slabs run one item per tile).
 void slab_plan(const sarbp_opts *opts, int precision, int nu, int nv, int *tile_x, int *tile_y,
                int *nslabs, int (&row0)[sarbp_ctx::kMaxSlabs + 1]) {
     Runner::tile_shape(opts, tile_x, tile_y);
     const int tiles_y = (nv + *tile_y - 1) / *tile_y;
     *nslabs = 0;
     if (precision == SARBP_PREC_NAIVE || (size_t)nu * nv < ((size_t)1 << 18) || tiles_y < 16) return;
+    if (opts && opts->pulse_parts >= 2) return;
     const int h0 = std::max(1, tiles_y / 32);
     const int rest = tiles_y - 4 * h0;  // after the first, second and last slabs
     const int nbody = std::max(1, std::min(sarbp_ctx::kMaxSlabs - 3, rest / 8));

@@ -34,9 +34,13 @@
 // each instance gets one arrival set from each side, and the producer
 // drains the last two EMPTY instances of every tile.
 //
-// Work list: items are (job, tile); with `persistent` the grid is the number
-// of resident CTAs and each CTA pulls items (ordered longest first by the
-// host) from an atomic counter, so uneven jobs of a batch share one launch.
+// Work list: items are (job, tile, pulse part); with `persistent` the grid
+// is the number of resident CTAs and each CTA pulls items (ordered longest
+// first by the host) from an atomic counter, so uneven jobs of a batch share
+// one launch.  A job with too few tiles to fill the resident CTAs has each
+// tile split into nsplit items over consecutive pulse ranges; each stores
+// its sums into its own slice of the job's parts buffer (plain stores, no
+// atomics), and the combine kernel adds the slices in a fixed order.
 //
 // Naive kernel: the same quantity with plain FP32 range |pos| - |r - pos|
 // and phase k_c * dr per pixel*pulse; kept as the precision-study baseline.
@@ -281,15 +285,17 @@ struct TileShape {
     int K, W, C, nchunks;
 };
 
-__device__ __forceinline__ TileShape tile_shape(const TileInfo &t, int P, int stage_cap, int cmax) {
+// Chunking of an item's np pulses: C pulses per chunk (the windows of a
+// chunk fill at most one staging half), nchunks chunks.
+__device__ __forceinline__ TileShape tile_shape(const TileInfo &t, int np, int stage_cap, int cmax) {
     TileShape s;
     s.K = t.K;
     s.W = 2 * t.K + 1;
     int C = stage_cap / s.W;
     if (C > cmax) C = cmax;
-    if (C > P) C = P;
+    if (C > np) C = np;
     s.C = C;
-    s.nchunks = C >= 1 ? (P + C - 1) / C : 0;
+    s.nchunks = C >= 1 ? (np + C - 1) / C : 0;
     return s;
 }
 
@@ -379,13 +385,15 @@ __device__ __forceinline__ void producer_loop(const DevJob *__restrict__ jobs,
         if (item >= nitems) break;
         const WorkItem wi = items[item];
         const DevJob &jb = jobs[wi.job];
-        const TileShape sh = tile_shape(jb.tiles[wi.tile], jb.P, stage_cap, cmax);
+        int pb, pe;  // the item's pulses
+        part_range(jb.P, jb.nsplit, wi.part, pb, pe);
+        const TileShape sh = tile_shape(jb.tiles[wi.tile], pe - pb, stage_cap, cmax);
         bool ok = true;
         for (int c = 0; c < sh.nchunks; ++c) {
             const int b = c & 1;
             if (c >= 2) bar_sync(kBarEmpty0 + b);  // consumers are done with chunk c-2
-            const int p0 = c * sh.C;
-            ok = stage_chunk(jb, wi.tile, lane, p0, min(sh.C, jb.P - p0), b, sh, stage_cap, cmax, sm, uses) &&
+            const int p0 = pb + c * sh.C;
+            ok = stage_chunk(jb, wi.tile, lane, p0, min(sh.C, pe - p0), b, sh, stage_cap, cmax, sm, uses) &&
                  ok;
             bar_arrive(kBarFull0 + b);
         }
@@ -432,7 +440,9 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
         const int tx0 = (wi.tile % jb.tiles_x) * TX;
         const int ty0 = (wi.tile / jb.tiles_x) * TY;
         const TileInfo ti = jb.tiles[wi.tile];
-        const TileShape sh = tile_shape(ti, P, stage_cap, cmax);
+        int pb, pe;  // the item's pulses
+        part_range(P, jb.nsplit, wi.part, pb, pe);
+        const TileShape sh = tile_shape(ti, pe - pb, stage_cap, cmax);
         const double k_c = jb.sc->k_c;
         const float kcf = (float)k_c;
 
@@ -490,9 +500,9 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
             for (int c = 0; c < sh.nchunks; ++c) {
                 const int b = c & 1;
                 bar_sync(kBarFull0 + b);
-                const int p0 = c * sh.C;
+                const int p0 = pb + c * sh.C;
                 const uint32_t poff = stage_base + (uint32_t)(b * stage_cap) * 16u;
-                const int nc = min(sh.C, P - p0);
+                const int nc = min(sh.C, pe - p0);
                 const float4 *rec2 = sm.rec2 + (size_t)b * 4 * cmax;
                 if (ti.wide)
                     accumulate_mode<true, NP, PRE>(sm.s_mode[b], ti.planar != 0, nc, rec2, poff, pstride, ILK, CL,
@@ -504,9 +514,20 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
             }
         }
         // ---- final phase, row flip (backprojection.cpp:130-138), max|z|;
-        // a pulse chunk adds its sums to the partial image instead ----
+        // a pulse part stores its sums into its slice, a pulse chunk adds
+        // them to the partial image instead ----
         double zmax = 0.0;
-        if (jb.acc) {
+        if (jb.nsplit > 1) {
+            float2 *slice = jb.parts + (long long)wi.part * ((long long)nu * nv);
+#pragma unroll
+            for (int k = 0; k < PPT; ++k) {
+                int ix, iy;
+                pixel_of(ti.transposed != 0, tx0, ty0, k, ix, iy);
+                if (ix < nu && iy < nv)
+                    slice[(long long)iy * nu + ix] = make_float2((k & 1) ? arp[k >> 1].y : arp[k >> 1].x,
+                                                                 (k & 1) ? aip[k >> 1].y : aip[k >> 1].x);
+            }
+        } else if (jb.acc) {
 #pragma unroll
             for (int k = 0; k < PPT; ++k) {
                 int ix, iy;
@@ -536,7 +557,7 @@ __device__ __forceinline__ void consumer_loop(const DevJob *__restrict__ jobs,
         zmax = warp_max(zmax);
         if (lane == 0) sm.sred[warp] = zmax;
         __syncthreads();
-        if (tid == 0 && !jb.acc) {
+        if (tid == 0 && !jb.acc && jb.nsplit <= 1) {
             double m = 0.0;
             for (int w = 0; w < kConsumerWarps; ++w) m = fmax(m, sm.sred[w]);
             atomicMax(&jb.sc->maxabs, (unsigned long long)__double_as_longlong(m));

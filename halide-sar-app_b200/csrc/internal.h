@@ -107,13 +107,32 @@ struct DevJob {
     // the backprojection adds its sums into acc instead of writing out
     int chunked;
     float2 *acc;          // [nv][nu] partial image (pixel-row order) or null
+    // pulse parts: a job whose tiles leave resident CTAs idle has each tile
+    // formed as nsplit items over consecutive pulse ranges (part_range);
+    // each item stores its sums into slice `part` of parts ([nsplit][nv][nu],
+    // pixel-row order), and the combine kernel adds the slices in order and
+    // applies the final phase.  nsplit <= 1: one item per tile.
+    int nsplit;
+    float2 *parts;
 };
 
-// (job, tile) work item of the per-tile kernels
+// (job, tile, pulse part) work item of the per-tile kernels
 struct WorkItem {
     int job;
     int tile;
+    int part;  // 0 .. nsplit - 1 (0 for the tile-geometry kernels)
 };
+
+// Pulses [p0, p1) of part `part` of nsplit near-equal parts of P.
+__host__ __device__ inline void part_range(int P, int nsplit, int part, int &p0, int &p1) {
+    if (nsplit <= 1) {
+        p0 = 0;
+        p1 = P;
+        return;
+    }
+    p0 = (int)((long long)part * P / nsplit);
+    p1 = (int)((long long)(part + 1) * P / nsplit);
+}
 
 // one row of a batched range-compression launch
 struct RowItem {

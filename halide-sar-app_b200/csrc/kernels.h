@@ -40,6 +40,7 @@ struct BpLaunch {
     int cmax;        // max pulses per chunk
     int persistent;  // 1: grid = resident CTAs pulling items from *counter
     int grid;        // CTAs when persistent
+    int parts;       // requested pulse parts per tile (sarbp_opts::pulse_parts)
 };
 bool bp_tile_supported(int tile_x, int tile_y, int minb);
 size_t bp_smem_bytes(const BpLaunch &L);
@@ -63,6 +64,10 @@ cudaError_t launch_chunk_tables(const double4 *pulse, const float *wP, int P, in
                                 float *wP_c, cudaStream_t st);
 cudaError_t launch_finalize(const DevJob *d_job, long long npix, int num_sms, cudaStream_t st);
 cudaError_t launch_fill_items(WorkItem *items, int ntiles, RowItem *rows, int nrows, cudaStream_t st);
+// jobs d_list[0 .. nlist) of d_jobs, formed in pulse parts: sum of the parts
+// times the final phase into out (row flip), max |z|
+cudaError_t launch_combine_parts(const DevJob *d_jobs, const int *d_list, int nlist, long long max_pixels,
+                                 int num_sms, cudaStream_t st);
 
 // resize.cu (the reference's data/resize.py resampling)
 struct ResizePlan {

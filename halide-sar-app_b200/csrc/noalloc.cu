@@ -118,13 +118,19 @@ int scratch_for_device(int dev, cudaStream_t st, void **addr, int *num_sms) {
 
 __global__ void store_job_kernel(DevJob dj, DevJob *dst) { *dst = dj; }
 
-// work items (0, t) for the job's tiles, range-compression rows (0, p), and
-// the persistent launch counter
-__global__ void init_items_kernel(WorkItem *items, int ntiles, RowItem *rows, int npulses, int *counter) {
+// work items (0, t, s) for the job's tiles and pulse parts (part 0 of every
+// tile first, which the tile-geometry kernel takes as its tile list),
+// range-compression rows (0, p), the persistent launch counter and the
+// combine kernel's job list
+__global__ void init_items_kernel(WorkItem *items, int ntiles, int nitems, RowItem *rows, int npulses,
+                                  int *counter, int *split_list) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < ntiles) items[t] = WorkItem{0, t};
+    if (t < nitems) items[t] = WorkItem{0, t % ntiles, t / ntiles};
     if (t < npulses) rows[t] = RowItem{0, t};
-    if (t == 0) *counter = 0;
+    if (t == 0) {
+        *counter = 0;
+        *split_list = 0;
+    }
 }
 
 __global__ void status_kernel(const JobScalars *sc, int *status) { *status = sc->status; }
@@ -165,16 +171,24 @@ extern "C" int sarbp_backprojection_noalloc(const sarbp_job *job, void *cuda_str
     if (!(lsb > lsa)) return bad("range axis is empty");
 
     // ---- scratch layout inside the static array ----
-    const BpLaunch L0 = default_launch(nullptr, 148);
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    const BpLaunch L0 = resolved_launch(nullptr, sms);
     const size_t P = (size_t)j.npulses, N = (size_t)j.n_fft, S = (size_t)j.nsamples;
     const int tiles_x = (j.nu + L0.tile_x - 1) / L0.tile_x, tiles_y = (j.nv + L0.tile_y - 1) / L0.tile_y;
     const size_t ntiles = (size_t)tiles_x * tiles_y;
+    // the pulse parts of the device entry point, so that both form the same image
+    const int nsplit = pulse_parts(j.nu, j.nv, j.npulses, L0, sms);
+    const size_t nitems = ntiles * (size_t)nsplit;
     int logN = 0;
     while ((1 << logN) < j.n_fft) ++logN;
     size_t o = kTwiddleBytes;  // the twiddle tables come first
     const size_t o_sc = o;    o = align_up(o + sizeof(JobScalars), 256);
     const size_t o_job = o;   o = align_up(o + sizeof(DevJob), 256);
-    const size_t o_items = o; o = align_up(o + ntiles * sizeof(WorkItem), 256);
+    const size_t o_items = o; o = align_up(o + nitems * sizeof(WorkItem), 256);
+    const size_t o_split = o; o = align_up(o + sizeof(int), 256);
     const size_t o_rows = o;  o = align_up(o + P * sizeof(RowItem), 256);
     const size_t o_cnt = o;   o = align_up(o + sizeof(int), 256);
     const size_t o_qp = o;    o = align_up(o + P * (N + 1) * sizeof(float4), 256);
@@ -185,14 +199,12 @@ extern "C" int sarbp_backprojection_noalloc(const sarbp_job *job, void *cuda_str
     const size_t o_tiles = o; o = align_up(o + ntiles * sizeof(TileInfo), 256);
     const size_t o_recs = o;  o = align_up(o + ntiles * P * sizeof(PulseRec), 256);
     const size_t o_fin = o;   o = align_up(o + (size_t)j.nu * j.nv * sizeof(float2), 256);
+    const size_t o_parts = o; o = align_up(o + (nsplit > 1 ? (size_t)nsplit * j.nu * j.nv * sizeof(float2) : 0), 256);
     if (o > kScratchBytes)
         return fail(SARBP_ERR_UNSUPPORTED,
                     "no-alloc: the job needs " + std::to_string(o >> 20) + " MiB of scratch, more than the " +
                         std::to_string(kScratchBytes >> 20) + " MiB static array");
 
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     void *base = nullptr;
     int num_sms = 0;
     cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
@@ -242,18 +254,21 @@ extern "C" int sarbp_backprojection_noalloc(const sarbp_job *job, void *cuda_str
     dj.out_u8 = j.out_u8;
     dj.dB_min = j.dB_min;
     dj.dB_max = j.dB_max;
+    dj.nsplit = nsplit;
+    dj.parts = nsplit > 1 ? reinterpret_cast<float2 *>(sb + o_parts) : nullptr;
 
     DevJob *d_job = reinterpret_cast<DevJob *>(sb + o_job);
     WorkItem *d_items = reinterpret_cast<WorkItem *>(sb + o_items);
     int *d_cnt = reinterpret_cast<int *>(sb + o_cnt);
     const float2 *d_tw = reinterpret_cast<const float2 *>(sb + twiddle_offset(logN));
     RowItem *d_rows = reinterpret_cast<RowItem *>(sb + o_rows);
+    int *d_split = reinterpret_cast<int *>(sb + o_split);
 
     // ---- launches (the prep kernel clears the job's scalars) ----
     store_job_kernel<<<1, 1, 0, st>>>(dj, d_job);
-    const size_t nfill = ntiles > P ? ntiles : P;
-    init_items_kernel<<<(int)((nfill + 255) / 256), 256, 0, st>>>(d_items, (int)ntiles, d_rows, j.npulses,
-                                                                  d_cnt);
+    const size_t nfill = nitems > P ? nitems : P;
+    init_items_kernel<<<(int)((nfill + 255) / 256), 256, 0, st>>>(d_items, (int)ntiles, (int)nitems, d_rows,
+                                                                  j.npulses, d_cnt, d_split);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "no-alloc set-up launches");
     launch_prep(d_job, 1, st);
@@ -263,8 +278,9 @@ extern "C" int sarbp_backprojection_noalloc(const sarbp_job *job, void *cuda_str
     BpLaunch L = L0;
     const int occ = bp_max_active_blocks(L);
     if (occ < 1) return fail(SARBP_ERR_CUDA, "no-alloc: backprojection kernel does not fit on an SM");
-    L.grid = (int)std::min<long long>((long long)occ * num_sms, (long long)ntiles);
-    e = launch_backproject(L, d_job, d_items, (int)ntiles, d_cnt, st);
+    L.grid = (int)std::min<long long>((long long)occ * num_sms, (long long)nitems);
+    e = launch_backproject(L, d_job, d_items, (int)nitems, d_cnt, st);
+    if (e == cudaSuccess && nsplit > 1) e = launch_combine_parts(d_job, d_split, 1, (long long)j.nu * j.nv, num_sms, st);
     if (e == cudaSuccess && j.out_u8) e = launch_batch_u8(d_job, 1, (long long)j.nu * j.nv, st);
     if (e == cudaSuccess && status) {
         status_kernel<<<1, 1, 0, st>>>(dj.sc, status);

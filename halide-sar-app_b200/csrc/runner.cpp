@@ -22,14 +22,15 @@ int ilog2i(long long n) {
 }
 
 struct JobLayout {
-    size_t Q, Qp, filt, wS, wP, pulse, tiles, recs, fin, end;
+    size_t Q, Qp, filt, wS, wP, pulse, tiles, recs, fin, parts, end;
 };
 
 // Scratch of one job: profiles (pairs for the tile kernel, plain Q for the
 // range-compression-only entry point), windows, pulse table, and for the
-// tile kernel the tile table, per-(tile, pulse) records and final phases.
+// tile kernel the tile table, per-(tile, pulse) records and final phases,
+// and for a job formed in nsplit > 1 pulse parts one partial image per part.
 JobLayout layout_of(const sarbp_job &j, size_t base, int tile_x, int tile_y, bool rc_only, bool naive,
-                    bool resident = false) {
+                    bool resident = false, int nsplit = 1) {
     JobLayout L;
     const size_t P = (size_t)j.npulses, N = (size_t)j.n_fft, S = (size_t)j.nsamples;
     const bool tiles = !rc_only && !naive;
@@ -45,6 +46,7 @@ JobLayout layout_of(const sarbp_job &j, size_t base, int tile_x, int tile_y, boo
     L.tiles = o;  o = align_up(o + ntiles * sizeof(TileInfo), 256);
     L.recs = o;   o = align_up(o + ntiles * P * sizeof(PulseRec), 256);
     L.fin = o;    o = align_up(o + (tiles ? (size_t)j.nu * j.nv * sizeof(float2) : 0), 256);
+    L.parts = o;  o = align_up(o + (tiles && nsplit > 1 ? (size_t)nsplit * j.nu * j.nv * sizeof(float2) : 0), 256);
     L.end = o;
     return L;
 }
@@ -131,6 +133,8 @@ void describe_job(const sarbp_job &j, int prec, int tile_x, int tile_y, DevJob &
     dj.dB_max = j.dB_max;
     dj.chunked = 0;
     dj.acc = nullptr;
+    dj.nsplit = 1;
+    dj.parts = nullptr;
 }
 
 void set_error(const std::string &msg) { g_error = msg; }
@@ -263,6 +267,7 @@ BpLaunch default_launch(const sarbp_opts *opts, int num_sms) {
     L.stage_cap = 2048;
     L.cmax = 64;
     L.persistent = 1;
+    L.parts = 0;
     if (opts) {
         if (opts->tile_x > 0 && opts->tile_y > 0) {
             L.tile_x = opts->tile_x;
@@ -272,17 +277,59 @@ BpLaunch default_launch(const sarbp_opts *opts, int num_sms) {
         L.persistent = opts->persistent == 2 ? 0 : 1;
         if (opts->stage_cap > 0) L.stage_cap = std::max(64, std::min(4096, opts->stage_cap)) & ~1;
         if (opts->min_blocks == 2 || opts->min_blocks == 3) L.minb = opts->min_blocks;
+        L.parts = std::max(0, std::min(16, opts->pulse_parts));
     }
     L.cmax = (L.cmax + 3) / 4 * 4;
     L.grid = num_sms;
     return L;
 }
 
-size_t Runner::job_scratch_bytes(const sarbp_job &j, const sarbp_opts *opts, bool resident_profiles) {
-    const BpLaunch L = default_launch(opts, 148);
+BpLaunch resolved_launch(const sarbp_opts *opts, int num_sms) {
+    BpLaunch L = default_launch(opts, num_sms);
+    if (!bp_tile_supported(L.tile_x, L.tile_y, L.minb) && !(opts && opts->min_blocks)) L.minb = 2;
+    return L;
+}
+
+int pulse_parts(int nu, int nv, int P, const BpLaunch &L, int num_sms) {
+    constexpr int kMaxParts = 16, kMinPartPulses = 32;
+    constexpr double kItemCost = 16.0;  // fixed cost of an item, in pulses of its tile
+    const long long ntiles = (long long)((nu + L.tile_x - 1) / L.tile_x) * ((nv + L.tile_y - 1) / L.tile_y);
+    const int sms = std::max(1, num_sms), minb = std::max(1, L.minb);
+    const long long R = (long long)minb * sms;  // resident CTAs
+    if (L.parts >= 1) return std::max(1, std::min(L.parts, P));
+    if ((long long)nu * nv >= (1ll << 18) || 2 * ntiles > R || ntiles < 1) return 1;
+    // Estimated time of s parts per tile, in pulse times of a CTA on a full
+    // SM: an SM running k CTAs does f(k) of a full SM's work (fewer warps
+    // hide less latency; measured on 256^2, 512^2 and 2048^2 images alone),
+    // and the SMs with the most items set the time.
+    auto f = [](long long k) { return k == 1 ? 0.80 : k == 2 ? 0.95 : 1.0; };
+    auto time_of = [&](int s) {
+        const long long items = ntiles * s;
+        const double item = (double)P / s + kItemCost;
+        if (items <= R) {
+            const long long k = (items + sms - 1) / sms;
+            return (double)k * item / f(k);
+        }
+        return (double)((items + R - 1) / R) * minb * item / f(minb);
+    };
+    int best = 1;
+    double best_t = time_of(1) / 1.15;
+    for (int s = 2; s <= kMaxParts && P / s >= kMinPartPulses; ++s) {
+        const double t = time_of(s);
+        if (t < best_t) {
+            best = s;
+            best_t = t;
+        }
+    }
+    return best;
+}
+
+size_t Runner::job_scratch_bytes(const sarbp_job &j, const sarbp_opts *opts, bool resident_profiles, int num_sms) {
+    const BpLaunch L = resolved_launch(opts, num_sms);
+    const bool naive = j.precision == SARBP_PREC_NAIVE;
+    const int ns = naive ? 1 : pulse_parts(j.nu, j.nv, j.npulses, L, num_sms);
     const size_t work = resident_profiles ? 0 : align_up(rc_work_bytes(ilog2i(j.n_fft)), 256);
-    return layout_of(j, 0, L.tile_x, L.tile_y, false, j.precision == SARBP_PREC_NAIVE, resident_profiles).end +
-           work;
+    return layout_of(j, 0, L.tile_x, L.tile_y, false, naive, resident_profiles, ns).end + work;
 }
 
 Runner::~Runner() {
@@ -321,9 +368,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
     }
     auto rec = [&](int i) { return (for_graph || !stage_events) ? cudaSuccess : dev_->record(i, st); };
     if (njobs < 1 || !jobs) return fail(SARBP_ERR_INVALID, "no jobs");
-    BpLaunch L = default_launch(opts, dev_->num_sms);
-    // a tile shape without a 3-CTA/SM build runs at 2 unless the caller asked
-    if (!bp_tile_supported(L.tile_x, L.tile_y, L.minb) && !(opts && opts->min_blocks)) L.minb = 2;
+    BpLaunch L = resolved_launch(opts, dev_->num_sms);
     if (!bp_tile_supported(L.tile_x, L.tile_y, L.minb))
         return fail(SARBP_ERR_INVALID, "unsupported pixel tile " + std::to_string(L.tile_x) + "x" +
                                            std::to_string(L.tile_y) + " at " + std::to_string(L.minb) +
@@ -338,11 +383,18 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         cudaError_t e = cudaEventCreateWithFlags(&meta_done_, cudaEventDisableTiming);
         if (e != cudaSuccess) return cuda_fail(e, "cudaEventCreate");
     }
+    // ---- pulse parts (row slabs come only for images of 2^18 pixels and
+    // more without a requested part count, which pulse_parts never splits) ----
+    std::vector<int> nsplit(njobs, 1);
+    for (int i = 0; i < njobs; ++i)
+        if (!rc_only && !slabs && prec[i] != SARBP_PREC_NAIVE)
+            nsplit[i] = pulse_parts(jobs[i].nu, jobs[i].nv, jobs[i].npulses, L, dev_->num_sms);
     // ---- scratch layout: JobScalars block first, then per-job arrays ----
     size_t off = align_up((size_t)njobs * sizeof(JobScalars), 256);
     std::vector<JobLayout> lay(njobs);
     for (int i = 0; i < njobs; ++i) {
-        lay[i] = layout_of(jobs[i], off, L.tile_x, L.tile_y, rc_only, prec[i] == SARBP_PREC_NAIVE, resident(i));
+        lay[i] = layout_of(jobs[i], off, L.tile_x, L.tile_y, rc_only, prec[i] == SARBP_PREC_NAIVE, resident(i),
+                           nsplit[i]);
         off = lay[i].end;
     }
     // work buffer of the four-step range compression (N_fft above
@@ -391,10 +443,11 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         return cudaMemcpyAsync(status_pin_.ptr, sbase, njobs * sizeof(JobScalars), cudaMemcpyDeviceToHost, st);
     };
 
-    // ---- rows grouped by N_fft, work items longest first ----
+    // ---- rows grouped by N_fft, work items longest first, one tile-geometry
+    // item per tile, the jobs formed in pulse parts ----
     std::map<int, std::vector<RowItem>> rows;
-    std::vector<WorkItem> items;
-    std::vector<int> naive;
+    std::vector<WorkItem> items, tiles;
+    std::vector<int> naive, split;
     for (int i = 0; i < njobs; ++i) {
         if (!resident(i)) {  // resident profiles were range-compressed before
             auto &v = rows[ilog2i(jobs[i].n_fft)];
@@ -407,19 +460,32 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         }
         const int tx = (jobs[i].nu + L.tile_x - 1) / L.tile_x;
         const int ty = (jobs[i].nv + L.tile_y - 1) / L.tile_y;
-        for (int t = 0; t < tx * ty; ++t) items.push_back(WorkItem{i, t});
+        for (int s = 0; s < nsplit[i]; ++s)
+            for (int t = 0; t < tx * ty; ++t) items.push_back(WorkItem{i, t, s});
+        if (nsplit[i] > 1) split.push_back(i);
     }
-    std::stable_sort(items.begin(), items.end(), [&](const WorkItem &a, const WorkItem &b) {
-        return jobs[a.job].npulses > jobs[b.job].npulses;
-    });
+    auto item_pulses = [&](const WorkItem &w) {
+        int p0, p1;
+        part_range(jobs[w.job].npulses, nsplit[w.job], w.part, p0, p1);
+        return p1 - p0;
+    };
+    std::stable_sort(items.begin(), items.end(),
+                     [&](const WorkItem &a, const WorkItem &b) { return item_pulses(a) > item_pulses(b); });
+    if (!split.empty())
+        for (const WorkItem &w : items)
+            if (w.part == 0) tiles.push_back(w);
     size_t nrows_total = 0;
     for (auto &kv : rows) nrows_total += kv.second.size();
 
-    // ---- meta block: [DevJob][RowItem...][WorkItem...][counter] ----
+    // ---- meta block: [DevJob][RowItem...][WorkItem...][tile WorkItem...]
+    // [split job...][counter] (the tile list only when a job is split: the
+    // work items are then not one per tile) ----
     const size_t o_jobs = 0;
     const size_t o_rows = align_up(o_jobs + (size_t)njobs * sizeof(DevJob), 256);
     const size_t o_items = align_up(o_rows + nrows_total * sizeof(RowItem), 256);
-    const size_t o_cnt = align_up(o_items + items.size() * sizeof(WorkItem), 256);
+    const size_t o_tiles = align_up(o_items + items.size() * sizeof(WorkItem), 256);
+    const size_t o_split = align_up(o_tiles + tiles.size() * sizeof(WorkItem), 256);
+    const size_t o_cnt = align_up(o_split + split.size() * sizeof(int), 256);
     const size_t meta_bytes = o_cnt + 256 * (size_t)(slabs ? slabs->nslabs : 1);
     if (for_graph && (host_meta_.cap < meta_bytes || meta_.cap < meta_bytes))
         return fail(SARBP_ERR_STATE, "graph capture needs a prior run of the same jobs");
@@ -451,6 +517,8 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         dj.wP = reinterpret_cast<float *>(sbase + lay[i].wP);
         dj.pulse = reinterpret_cast<double4 *>(sbase + lay[i].pulse);
         dj.sc = reinterpret_cast<JobScalars *>(sbase) + i;
+        dj.nsplit = nsplit[i];
+        dj.parts = nsplit[i] > 1 ? reinterpret_cast<float2 *>(sbase + lay[i].parts) : nullptr;
     }
     RowItem *hr = reinterpret_cast<RowItem *>(h + o_rows);
     std::vector<std::pair<int, size_t>> row_groups;  // (logN, first row)
@@ -461,6 +529,8 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         rpos += kv.second.size();
     }
     std::memcpy(h + o_items, items.data(), items.size() * sizeof(WorkItem));
+    std::memcpy(h + o_tiles, tiles.data(), tiles.size() * sizeof(WorkItem));
+    std::memcpy(h + o_split, split.data(), split.size() * sizeof(int));
 
     cudaStream_t ms = (slabs && slabs->copy_stream) ? slabs->copy_stream : st;
     e = cudaMemcpyAsync(d, h, meta_bytes, cudaMemcpyHostToDevice, ms);
@@ -472,6 +542,9 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
     const DevJob *d_jobs = reinterpret_cast<const DevJob *>(d + o_jobs);
     const RowItem *d_rows = reinterpret_cast<const RowItem *>(d + o_rows);
     const WorkItem *d_items = reinterpret_cast<const WorkItem *>(d + o_items);
+    const WorkItem *d_tiles = split.empty() ? d_items : reinterpret_cast<const WorkItem *>(d + o_tiles);
+    const int ntile_items = split.empty() ? (int)items.size() : (int)tiles.size();
+    const int *d_split = reinterpret_cast<const int *>(d + o_split);
     int *d_cnt = reinterpret_cast<int *>(d + o_cnt);
 
     // twiddle tables first (a one-time synchronous upload per N_fft; a
@@ -582,7 +655,7 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         items.clear();  // formed above
     }
     if (!items.empty()) {
-        e = launch_tile_setup(d_jobs, d_items, (int)items.size(), L.tile_x * L.tile_y, st);
+        e = launch_tile_setup(d_jobs, d_tiles, ntile_items, L.tile_x * L.tile_y, st);
         if (e != cudaSuccess) return cuda_fail(e, "tile geometry launch");
         dev_->launches += 1;
     }
@@ -596,6 +669,13 @@ int Runner::enqueue(const sarbp_job *jobs, int njobs, const sarbp_opts *opts, cu
         }
         e = launch_backproject(L, d_jobs, d_items, (int)items.size(), d_cnt, st);
         if (e != cudaSuccess) return cuda_fail(e, "backprojection launch");
+        dev_->launches++;
+    }
+    if (!split.empty()) {
+        long long px = 0;
+        for (int i : split) px = std::max(px, (long long)jobs[i].nu * jobs[i].nv);
+        e = launch_combine_parts(d_jobs, d_split, (int)split.size(), px, dev_->num_sms, st);
+        if (e != cudaSuccess) return cuda_fail(e, "pulse-part combine launch");
         dev_->launches++;
     }
     for (int i : naive) {

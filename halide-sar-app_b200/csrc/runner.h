@@ -122,9 +122,10 @@ public:
     static void tile_shape(const sarbp_opts *opts, int *tile_x, int *tile_y);
     // Waits for the last batch and reads the kernels' status words.
     int check_status(cudaStream_t st);
-    // Device footprint of the library scratch a job needs (bytes).
+    // Device footprint of the library scratch a job needs (bytes) on a GPU
+    // of num_sms SMs.
     static size_t job_scratch_bytes(const sarbp_job &j, const sarbp_opts *opts = nullptr,
-                                    bool resident_profiles = false);
+                                    bool resident_profiles = false, int num_sms = 148);
     // Frees the scratch (the Runner must be idle).
     void release_scratch() { scratch_.release(); }
     // Take each batch's scratch from `pool` (stream-ordered) instead of the
@@ -152,6 +153,19 @@ private:
 };
 
 BpLaunch default_launch(const sarbp_opts *opts, int num_sms);
+// default_launch with the CTAs per SM the enqueue uses: a tile shape without
+// a 3-CTA/SM build runs at 2 unless the caller asked
+BpLaunch resolved_launch(const sarbp_opts *opts, int num_sms);
+
+// Pulse parts per tile of a one-shot job (DevJob::nsplit): L.parts when the
+// caller set it (at most one part per pulse); otherwise 1 for images of
+// 2^18 pixels and more and for jobs whose tiles fill more than half of the
+// resident CTAs, and else the part count with the best estimated use of
+// the SMs (whole waves of equal items, a fixed cost per item), each part at
+// least 32 pulses, at most 16 parts, and 1 unless that beats one item per
+// tile by 15 %.  Depends only on the job's sizes, the launch shape and the
+// SM count, so a job splits the same way alone and in any batch.
+int pulse_parts(int nu, int nv, int P, const BpLaunch &L, int num_sms);
 
 // Checks a job's sizes, pointers and Taylor level (SARBP_OK or an error code
 // with the message set); need_phs = false for pulse-chunked jobs, whose

@@ -101,7 +101,7 @@ def pixel_locs(u, v, u_hat, v_hat):
     return out
 
 
-def _opts(precision=None, tile=None, pulse_chunk=0, persistent=0, stage_cap=0, min_blocks=0):
+def _opts(precision=None, tile=None, pulse_chunk=0, persistent=0, stage_cap=0, min_blocks=0, pulse_parts=0):
     o = Opts()
     o.precision = PREC_COMPAT if precision is None else int(precision)
     if tile:
@@ -110,6 +110,7 @@ def _opts(precision=None, tile=None, pulse_chunk=0, persistent=0, stage_cap=0, m
     o.persistent = int(persistent)
     o.stage_cap = int(stage_cap)
     o.min_blocks = int(min_blocks)
+    o.pulse_parts = int(pulse_parts)
     return o
 
 
@@ -294,7 +295,7 @@ class Context:
         ms = ctypes.c_float()
         check(lib().sarbp_autotune(self._h, arr, len(jobs), ctypes.byref(o), ctypes.byref(ms)))
         tune = dict(tile=(o.tile_x, o.tile_y), pulse_chunk=o.pulse_chunk, min_blocks=o.min_blocks,
-                    stage_cap=o.stage_cap)
+                    stage_cap=o.stage_cap, pulse_parts=o.pulse_parts)
         return tune, ms.value
 
     def plan(self, jobs, precision=None, **tune):

@@ -40,7 +40,7 @@ class SarbpError(RuntimeError):
 class Opts(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("tile_x", ctypes.c_int), ("tile_y", ctypes.c_int),
                 ("pulse_chunk", ctypes.c_int), ("persistent", ctypes.c_int),
-                ("stage_cap", ctypes.c_int), ("min_blocks", ctypes.c_int), ("reserved", ctypes.c_int)]
+                ("stage_cap", ctypes.c_int), ("min_blocks", ctypes.c_int), ("pulse_parts", ctypes.c_int)]
 
 
 class Job(ctypes.Structure):

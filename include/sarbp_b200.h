@@ -75,7 +75,11 @@ typedef struct sarbp_opts {
     int persistent;  /* 0 or 1: persistent work-list launch; 2: one CTA per tile */
     int stage_cap;   /* float4 entries of each half of the range-window staging buffer */
     int min_blocks;  /* CTAs per SM the kernel's registers are sized for (2 or 3) */
-    int reserved;
+    int pulse_parts; /* work items per pixel tile over consecutive pulse ranges: 0 = chosen
+                        per job (images below 2^18 pixels whose tiles leave resident CTAs
+                        idle are split; the parts' sums are added in a fixed order, so a
+                        job forms the same image alone and in any batch), 1 = one item
+                        per tile, 2..16 = that many parts (at most one per pulse) */
 } sarbp_opts;
 
 /*

@@ -121,3 +121,25 @@ def test_errors_without_gpu_are_codes(sb):
     with pytest.raises(sb.SarbpError) as ei:
         sb.Context(0)
     assert ei.value.code in (sb._lib.ERR_CUDA, sb._lib.ERR_INVALID)
+
+
+def test_pulse_parts_in_the_job_footprint(sb):
+    """Small one-shot jobs are formed in pulse parts (one partial image per
+    part in the footprint); images of 2^18 pixels and more are not unless
+    asked; an explicit part count applies to any image."""
+    def fp(nu, nv, P, **tune):
+        job = sb.make_job(1024, P, 4096, 30, nu, nv, 0.2, 0, 0, 0, 0, r=1)
+        return sb.job_device_bytes(job, precision=sb.PREC_COMPAT, **tune)
+    # 256^2: 64 tiles of 32x32 for 148 SMs x 3 resident CTAs -> 4 parts of
+    # 125 pulses (two items on each of 128 SMs)
+    assert fp(256, 256, 500) - fp(256, 256, 500, pulse_parts=1) == 4 * 256 * 256 * 8
+    # 100 pulses: 2 parts (one item on each of 128 SMs); 40: no part of 32
+    # pulses pays for its fixed cost
+    assert fp(256, 256, 100) - fp(256, 256, 100, pulse_parts=1) == 2 * 256 * 256 * 8
+    assert fp(256, 256, 40) == fp(256, 256, 40, pulse_parts=1)
+    # 2048^2 (4096 tiles) and 512^2 (2^18 pixels): one item per tile
+    assert fp(2048, 2048, 1999) == fp(2048, 2048, 1999, pulse_parts=1)
+    assert fp(512, 512, 469) == fp(512, 512, 469, pulse_parts=1)
+    # explicit parts: 4 partial images of 2048^2, capped at one part per pulse
+    assert fp(2048, 2048, 1999, pulse_parts=4) - fp(2048, 2048, 1999) == 4 * 2048 * 2048 * 8
+    assert fp(64, 64, 3, pulse_parts=16) - fp(64, 64, 3, pulse_parts=1) == 3 * 64 * 64 * 8

@@ -295,6 +295,33 @@ def test_tile_shapes_agree(ctx, oracle, cfg1, tile):
     assert rel_l2(img, ref) < REL_COMPAT
 
 
+@pytest.mark.parametrize("parts", [0, 3, 7, 16])
+def test_pulse_parts_match_one_item_per_tile(ctx, oracle, parts):
+    """Tiles formed as several (tile, pulse part) work items, each part's
+    sums stored in its own partial image and added in part order by the
+    combine kernel (0: the part count chosen for the job, here 4 for 64
+    tiles and 469 pulses).  Near field (400 m): wide tiles, series orders 1
+    to 3, odd P (the fftshifted pulse axis), P not a multiple of the part
+    count.  Against one item per tile: relative L2 <= 1e-5 (the same terms
+    summed in another order, and a chunk's series order taken over other
+    pulses); against the oracle at the compat tolerance."""
+    from sarbp_b200 import synth
+    d = synth.make("plain_small", seed=3, overrides=dict(R0=400.0, extent=120.0, n=256, upsample=2))
+    pos32, k32 = d["pos"].astype(np.float32), d["k_r"].astype(np.float32)
+    run = lambda **kw: ctx.backprojection_cuda(d["phs"], k32, d["taylor"], d["N_fft"], d["delta_r"], d["u"],
+                                               d["v"], pos32, d["r"], **kw)
+    one = run(pulse_parts=1)
+    img = run(pulse_parts=parts)
+    assert np.array_equal(img, run(pulse_parts=parts))  # deterministic
+    ref = oracle.backprojection(d["phs"], k32, d["taylor"], d["N_fft"], d["delta_r"], pos32, d["r"],
+                                d["nu"], d["nv"], mode=oracle.MODE_REF)
+    e_one, e_ref = rel_l2(img, one), rel_l2(img, ref)
+    print("pulse parts %d: rel-L2 vs one item per tile %.3e, vs oracle %.3e" % (parts, e_one, e_ref))
+    assert 0 < e_one < 1e-5
+    assert e_ref < REL_COMPAT
+    assert db_max_diff(img, ref, d["db"][0]) < DB_TOL
+
+
 @pytest.mark.parametrize("chunk,persistent", [(4, 0), (16, 2), (64, 2), (256, 1)])
 def test_pulse_chunk_and_launch_modes(ctx, oracle, cfg1, chunk, persistent):
     d = cfg1
