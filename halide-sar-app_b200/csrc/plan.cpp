@@ -4,7 +4,8 @@
 // enqueued once for real, which sizes every scratch buffer and builds the
 // twiddle tables, and then captured into a CUDA graph: prep, one range
 // compression launch per FFT length, tile geometry, the persistent
-// backprojection over the (job, tile) work list and the u8 stage.  Each
+// backprojection over the (job, tile, pulse part) work list (and the combine
+// of pulse parts) and the u8 stage.  Each
 // replay re-reads the job descriptors from the plan's own pinned copy, so the
 // input arrays may hold new data between replays but must keep their
 // addresses and shapes.
