@@ -349,7 +349,8 @@ def test_two_ctas_with_grown_staging(ctx, oracle, cfg1, tile, chunk, stage):
 @pytest.mark.parametrize("P,S,nu,nv", [(2, 2, 1, 1), (3, 17, 7, 13), (64, 100, 33, 65), (200, 50, 100, 3)])
 def test_ragged_sizes(ctx, oracle, P, S, nu, nv):
     """Tiny and ragged shapes: edge tiles, P and S far from powers of two,
-    N_fft below S (the pulse centre is kept)."""
+    N_fft below S (the pulse centre is kept); also with 16 pulse parts per
+    tile requested (one part per pulse when P < 16)."""
     from sarbp_b200 import synth
     scat = synth.scene(4, 5.0, 0, seed=P)
     phs, pos, k_r = synth.phase_history(S, P, 9.3e9, 2e6, 9e3, 35, 3, scat, 30.0, P + S)
@@ -358,11 +359,13 @@ def test_ragged_sizes(ctx, oracle, P, S, nu, nv):
     u, v = g["u"][:nu], g["v"][:nv]
     r = synth.pixel_locs(u, v, g["u_hat"], g["v_hat"])
     for N in (16, 64):
-        img = ctx.backprojection_cuda(phs, k_r.astype(np.float32), 17, N, dr, u, v, pos.astype(np.float32), r)
         ref = oracle.backprojection(phs, k_r.astype(np.float32), 17, N, dr, pos.astype(np.float32), r,
                                     nu, nv, mode=oracle.MODE_REF)
-        assert img.shape == (nv, nu)
-        assert rel_l2(img, ref) < 5 * REL_COMPAT
+        for parts in (0, 16):
+            img = ctx.backprojection_cuda(phs, k_r.astype(np.float32), 17, N, dr, u, v, pos.astype(np.float32), r,
+                                          pulse_parts=parts)
+            assert img.shape == (nv, nu)
+            assert rel_l2(img, ref) < 5 * REL_COMPAT
 
 
 def test_scattered_pixels(ctx, oracle, cfg1):
