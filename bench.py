@@ -18,6 +18,11 @@ per-pixel pulse accumulation into the complex128 image, all on the device.
 Multi-GPU (torchrun, N > 1): every rank forms its own image (replicas, weak
 scaling); the time is the max over ranks.
 
+Other configurations (own JSON line each): --config batch96 (the batched
+form), --config serve (the serving sweep), --config cli_sandia (the sarbp
+CLI end to end with the reference's one-node Sandia command line, beside the
+stage times of that run's log), and any synth configuration name.
+
 --impl reference times the reference algorithm's CPU implementation (the
 C restatement in oracle/, reference precision, all host threads) on a
 bounded pixel sample of the same workload; only rank 0 runs it.
@@ -935,6 +940,114 @@ def run_serve(args, rank, world, local_rank):
         print(json.dumps(out), flush=True)
 
 
+# The reference's one-node Sandia run (exp/summit/darpa-demo2): its command
+# line and the stage times its log reports, on 1 Summit node (2x POWER9, the
+# CPU schedule, 42 and then 168 host threads).
+SANDIA1_CMD = ["-d", "-45.0", "-D", "0.0", "-t", "30", "-u", "2"]
+SANDIA1_PUBLISHED = {
+    "hardware": "1 Summit node, 2x POWER9, the reference's -s cpu schedule (42 threads, then 168)",
+    "data": "the Sandia phase history (1999 pulses x 1800 samples; not shipped with the reference)",
+    "source": "exp/summit/darpa-demo2/logs/SARBP-Sandia-1.763157:182-201",
+    "load_ms": 181, "image_plane_ms": 139, "backprojection_ms": [35528, 17448],
+    "dB_ms": 41, "u8_ms": 16, "png_write_ms": 421,
+}
+
+
+def write_platform_dir(d, data):
+    """A platform directory in the reference's .npy layout (PlatformData.cpp:
+    phs complex128 [P][S], pos f32 [P][3], k_r f64 [S], delta_r, R_c f32 (the
+    mid-aperture antenna position), npulses, nsamples) with the element
+    types the Sandia run's log shows (the CLI downcasts phs and k_r)."""
+    os.makedirs(d, exist_ok=True)
+    P, S = data["phs"].shape
+    np.save(os.path.join(d, "phs.npy"), data["phs"].astype(np.complex128))
+    np.save(os.path.join(d, "pos.npy"), np.ascontiguousarray(data["pos"], np.float32))
+    np.save(os.path.join(d, "k_r.npy"), np.ascontiguousarray(data["k_r"], np.float64))
+    np.save(os.path.join(d, "delta_r.npy"), np.array(float(data["delta_r"])))
+    np.save(os.path.join(d, "R_c.npy"), np.ascontiguousarray(data["pos"][P // 2], np.float32))
+    np.save(os.path.join(d, "npulses.npy"), np.array(P, np.int64))
+    np.save(os.path.join(d, "nsamples.npy"), np.array(S, np.int64))
+    return d
+
+
+def run_cli(args, rank, world, local_rank):
+    """--config cli_sandia: the sarbp CLI end to end with the reference's
+    one-node Sandia command line (-d -45 -D 0 -t 30 -u 2) on a seeded
+    synthetic platform directory of that run's shape (1999 pulses x 1800
+    samples; the CLI's image plane is then 2048^2 and N_fft 4096): load,
+    image plane, `steps` + 1 backprojection calls from host buffers (the
+    first one also creates the context), dB, u8 and the PNG write, each
+    from the CLI's own progress lines, beside the times the reference's log
+    reports for the same command on its Sandia data."""
+    import re
+    import shutil
+    import tempfile
+    import torch
+    from sarbp_b200 import synth
+
+    sarbp = os.path.join(ROOT, "halide-sar-app_b200", "bin", "sarbp")
+    if not os.path.exists(sarbp):
+        raise SystemExit("sarbp CLI not built (make -C halide-sar-app_b200)")
+    data = synth.make("sandia_2048", seed=2 + rank, with_r=False)
+    P, S = data["phs"].shape
+    tmp = tempfile.mkdtemp(prefix="sarbp_cli_")
+    try:
+        pdir = write_platform_dir(os.path.join(tmp, "sandia"), data)
+        iters = 1 + max(1, min(args.steps, 20))
+        env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank)))
+        clocks = Clocks(gpu_uuid(torch, torch.device("cuda", local_rank)))
+        clocks.start()
+        t0 = time.perf_counter()
+        p = subprocess.run([sarbp, "-p", pdir, "-o", os.path.join(tmp, "sandia.png")] + SANDIA1_CMD +
+                           ["-n", str(iters)], capture_output=True, text=True, timeout=600, env=env)
+        wall = time.perf_counter() - t0
+        clk = clocks.stop()
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    if p.returncode != 0:
+        raise SystemExit("sarbp failed (%d): %s" % (p.returncode, p.stdout[-2000:] + p.stderr[-2000:]))
+    out = p.stdout
+    ms = lambda pat: [float(x) for x in re.findall(pat, out)]
+    bp = ms(r"\(\d+\) Halide backprojection returned 0 in ([0-9.]+) ms")
+    nu = int(re.search(r"X length: (\d+)", out).group(1))
+    nv = int(re.search(r"Y length: (\d+)", out).group(1))
+    warm = bp[1:]
+    med = statistics.mean(warm)  # the lines give whole milliseconds: the mean resolves finer
+    rate = lambda t: nu * nv * P / (t * 1e-3) / 1e9
+    pub = SANDIA1_PUBLISHED
+    stages = {"load": ms(r"Loaded platform data in ([0-9.]+) ms")[0],
+              "image_plane": ms(r"Computed image plane parameters in ([0-9.]+) ms")[0],
+              "backprojection_first": bp[0], "backprojection_warm": warm,
+              "dB": ms(r"Halide dB conversion returned 0 in ([0-9.]+) ms")[0],
+              "u8": ms(r"Halide PNG production returned 0 in ([0-9.]+) ms")[0],
+              "png_write": ms(r"Wrote .* in ([0-9.]+) ms")[0]}
+    h2d = P * S * 8 + P * 12 + S * 4 + (nu + nv) * 8
+    res = {
+        "metric": "Gpixel*pulses/s (sarbp CLI backprojection call, %dx%d image, %d pulses x %d samples)"
+                  % (nu, nv, P, S),
+        "value": rate(med), "unit": "Gpixel*pulses/s", "n_gpus": 1, "steps": len(warm), "warmup": 1,
+        "ms_per_step": med, "higher_is_better": True, "scaling": "weak",
+        # the faster of the two published calls (168 threads)
+        "vs_baseline": rate(med) / rate(min(pub["backprojection_ms"])),
+        "dtype": "f32 (split-precision; f64 per-pulse set-up, the reference's f32 positions)",
+        "data": "synthetic (seeded; the Sandia run's shapes; complex128/f64 platform files as the Sandia data)",
+        "config": {"workload": "cli_sandia: sarbp %s on %d pulses x %d samples -> %dx%d image, N_fft %d"
+                               % (" ".join(SANDIA1_CMD), P, S, nu, nv, n_fft_of(S, 2)),
+                   "parallelism": "replicas1", "l2": "host buffers; each call copies its inputs and image"},
+        "e2e": {"value": rate(med), "unit": "Gpixel*pulses/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": nu * nv * 16},
+        "stages_ms": stages, "cli_wall_s": wall,
+        "published_reference": dict(pub, backprojection_gpix_pulses_s=[rate(t) for t in pub["backprojection_ms"]]),
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+
+
+def n_fft_of(S, u):
+    return int(math.pow(2, int(math.log2(S * u)) + 1))  # sarbp.cpp:258
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -962,6 +1075,8 @@ def main():
                 run_batch(args, rank, world, local_rank)
             elif args.config == "serve":
                 run_serve(args, rank, world, local_rank)
+            elif args.config == "cli_sandia":
+                run_cli(args, rank, world, local_rank)
             else:
                 run_ours(args, rank, world, local_rank)
     finally:

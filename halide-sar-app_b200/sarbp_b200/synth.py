@@ -14,6 +14,9 @@ and geometry scale:
   plain_mid    plain_large's aperture on a 1024^2 image over 50 m
   precision    4000 x 2048 at 20 km, 300 scatterers, 4096^2 image
   sandia_8192  8192 x 8192 (the reference's Sandia 8192^2 runs), 8192^2 over 400 m
+  sandia_2048  1999 x 1800 (the reference's one-node Sandia run, whose CLI
+               forms a 2048^2 image over the 254 m range swath), 200
+               scatterers in +-100 m
   batch        96 uneven jobs (image 256^2..2048^2, 128-2000 pulses,
                256/512/1024 samples, Taylor 17-35 dB, 5-15 km, 20-50 deg)
 
@@ -49,6 +52,9 @@ CONFIGS = {
     # range swath (2 km) covers a 8192^2 image over 400 m
     "sandia_8192": dict(P=8192, S=8192, f0=16.7e9, df=0.59e6 / 8, R0=8e3, dep=45.0, span=3.0,
                         nscat=60, half=180.0, clutter=0, snr=20.0, n=8192, extent=400.0,
+                        taylor=30, upsample=2, db=(-45.0, 0.0)),
+    "sandia_2048": dict(P=1999, S=1800, f0=16.7e9, df=0.59e6, R0=8e3, dep=45.0, span=3.0,
+                        nscat=200, half=100.0, clutter=0, snr=20.0, n=2048, extent=254.0,
                         taylor=30, upsample=2, db=(-45.0, 0.0)),
 }
 
