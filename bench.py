@@ -21,7 +21,9 @@ scaling); the time is the max over ranks.
 Other configurations (own JSON line each): --config batch96 (the batched
 form), --config serve (the serving sweep), --config cli_sandia (the sarbp
 CLI end to end with the reference's one-node Sandia command line, beside the
-stage times of that run's log), and any synth configuration name.
+stage times of that run's log), --config streamed (a 4096^2 x 4000 image
+formed in pulse chunks under a device-memory cap), and any synth
+configuration name.
 
 --impl reference times the reference algorithm's CPU implementation (the
 C restatement in oracle/, reference precision, all host threads) on a
@@ -59,6 +61,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="plain_large")
+    ap.add_argument("--cap-gb", type=float, default=1.25, help="--config streamed: device-memory cap (GB)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="CPU work of the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1044,6 +1047,95 @@ def run_cli(args, rank, world, local_rank):
         print(json.dumps(res), flush=True)
 
 
+def run_streamed(args, rank, world, local_rank):
+    """--config streamed: one 4096^2 image from 4000 pulses x 2048 samples
+    (N_fft 8192, 20 km, PREC_PRECISE) in host memory, formed by
+    sarbp_backprojection_streamed under a device-memory cap smaller than
+    its one-shot footprint (pulse chunks into a device-resident partial
+    image, each chunk's rows uploaded under the previous chunk's kernels),
+    against the same call with no cap (one chunk) and the device-resident
+    one-shot call of the same job.  Host buffers are pinned; the streamed
+    calls' wall time includes their copies and device allocations."""
+    import torch
+    import sarbp_b200 as sb
+    from sarbp_b200 import synth
+    from sarbp_b200.batch import HostJob
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    pin = lambda shape, dtype: torch.empty(shape, dtype=getattr(torch, np.dtype(dtype).name)).pin_memory().numpy()
+    cfg = dict(synth.CONFIGS["precision"], nscat=40, clutter=0)
+    d = synth.make("precision", seed=5 + rank, with_r=False, overrides=cfg)
+    hj = HostJob(dict(cfg, seed=5 + rank), alloc=pin, data=d)
+    out = hj.new_outputs()[0]
+    job = hj.job(out, precision=sb.PREC_PRECISE)
+    units = hj.units
+    cap = float(args.cap_gb) * 1e9
+    ctx = sb.Context(local_rank)
+    clocks = Clocks(gpu_uuid(torch, dev))
+    res = {}
+    try:
+        one_shot = sb.job_device_bytes(job, precision=sb.PREC_PRECISE)
+
+        def timed(max_bytes):
+            for _ in range(args.warmup):
+                C, used = sb.backprojection_streamed(ctx, job, max_bytes, precision=sb.PREC_PRECISE)
+            ts = []
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                C, used = sb.backprojection_streamed(ctx, job, max_bytes, precision=sb.PREC_PRECISE)
+                ts.append(time.perf_counter() - t0)
+            return C, used, statistics.median(ts)
+
+        clocks.start()
+        C, used, t_cap = timed(cap)
+        C1, used1, t_one = timed(1e15)
+        # the one-shot call with inputs resident on the device
+        dv = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        t = dict(phs=dv(d["phs"].view(np.float32)), k=dv(d["k_r"].astype(np.float32)),
+                 pos=dv(d["pos"].astype(np.float32)), k64=dv(d["k_r"]), pos64=dv(d["pos"]),
+                 u=dv(d["u"]), v=dv(d["v"]))
+        o = torch.empty((d["nv"], d["nu"], 2), dtype=torch.float64, device=dev)
+        jd = sb.make_job(d["S"], d["P"], d["N_fft"], d["taylor"], d["nu"], d["nv"], d["delta_r"],
+                         t["phs"].data_ptr(), t["k"].data_ptr(), t["pos"].data_ptr(), o.data_ptr(),
+                         u=t["u"].data_ptr(), v=t["v"].data_ptr(), u_hat=d["u_hat"], v_hat=d["v_hat"],
+                         k_r64=t["k64"].data_ptr(), pos64=t["pos64"].data_ptr(), precision=sb.PREC_PRECISE)
+        for _ in range(args.warmup):
+            ctx.run_jobs([jd])
+        ctx.synchronize()
+        ts = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            ctx.run_jobs([jd])
+            ctx.synchronize()
+            ts.append(time.perf_counter() - t0)
+        t_dev = statistics.median(ts)
+        clk = clocks.stop()
+    finally:
+        ctx.close()
+    rate = lambda sec: units / sec / 1e9
+    res = {
+        "metric": "Gpixel*pulses/s (4096^2 image, 4000 pulses, formed under a %.2f GB device-memory cap)"
+                  % (cap / 1e9),
+        "value": rate(t_cap), "unit": "Gpixel*pulses/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_cap * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (split-precision; f64 per-pulse set-up, PREC_PRECISE)",
+        "data": "synthetic (seeded; 40 scatterers at 20 km)",
+        "config": {"workload": "streamed: 4096x4096 image, 4000 pulses x 2048 samples, N_fft 8192, "
+                               "host buffers (pinned), cap %.2f GB" % (cap / 1e9),
+                   "parallelism": "replicas1", "l2": "inputs and outputs > 126 MB L2, no flush"},
+        "e2e": {"value": rate(t_cap), "unit": "Gpixel*pulses/s",
+                "h2d_bytes_per_step": hj.phs.nbytes + hj.k64.nbytes + hj.p64.nbytes + hj.u.nbytes + hj.v.nbytes,
+                "d2h_bytes_per_step": out.nbytes},
+        "chunk_pulses": C, "device_bytes_held": used, "one_shot_device_bytes": one_shot,
+        "no_cap": {"chunk_pulses": C1, "device_bytes_held": used1, "ms": t_one * 1e3, "rate": rate(t_one)},
+        "device_resident_one_shot": {"ms": t_dev * 1e3, "rate": rate(t_dev)},
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+
+
 def n_fft_of(S, u):
     return int(math.pow(2, int(math.log2(S * u)) + 1))  # sarbp.cpp:258
 
@@ -1077,6 +1169,8 @@ def main():
                 run_serve(args, rank, world, local_rank)
             elif args.config == "cli_sandia":
                 run_cli(args, rank, world, local_rank)
+            elif args.config == "streamed":
+                run_streamed(args, rank, world, local_rank)
             else:
                 run_ours(args, rank, world, local_rank)
     finally:
