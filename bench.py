@@ -22,8 +22,9 @@ Other configurations (own JSON line each): --config batch96 (the batched
 form), --config serve (the serving sweep), --config cli_sandia (the sarbp
 CLI end to end with the reference's one-node Sandia command line, beside the
 stage times of that run's log), --config streamed (a 4096^2 x 4000 image
-formed in pulse chunks under a device-memory cap), and any synth
-configuration name.
+formed in pulse chunks under a device-memory cap), --config resize (the
+data/resize.py resampling on the device beside its scipy restatement), and
+any synth configuration name.
 
 --impl reference times the reference algorithm's CPU implementation (the
 C restatement in oracle/, reference precision, all host threads) on a
@@ -1136,6 +1137,92 @@ def run_streamed(args, rank, world, local_rank):
         print(json.dumps(res), flush=True)
 
 
+def run_resize(args, rank, world, local_rank):
+    """--config resize: the reference's data/resize.py resampling of a phase
+    history of the one-node Sandia run's shape (1999 x 1800 complex128) to
+    twice and to half its pulse and sample counts (resize.py -p 2 -s 2 and
+    -p 0.5 -s 0.5), on the device (sarbp_resize_device, the real and
+    imaginary parts as two interleaved f64 components; CUDA events on the
+    context's stream), beside skimage's resize as restated on scipy in
+    oracle/resize_oracle.py (host, one call per part), which also checks
+    the device result.  HBM roofline on the input read plus the output
+    written once."""
+    import torch
+    import sarbp_b200 as sb
+    from sarbp_b200 import synth
+    from sarbp_b200._lib import lib, check
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import resize_oracle as RO
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    d = synth.make("sandia_2048", seed=2 + rank, with_r=False)
+    phs = d["phs"].astype(np.complex128)
+    P, S = phs.shape
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    ctx = sb.Context(local_rank)
+    st = torch.cuda.current_stream()
+    ctx.set_stream(st.cuda_stream)
+    cases = []
+    try:
+        src = torch.from_numpy(phs.view(np.float64)).to(dev)
+        for name, (po, so) in (("up2 (-p 2 -s 2)", (2 * P, 2 * S)), ("down2 (-p 0.5 -s 0.5)", (P // 2, S // 2))):
+            dst = torch.empty((po, 2 * so), dtype=torch.float64, device=dev)
+
+            def call():
+                check(lib().sarbp_resize_device(ctx.handle, 8, 2, ctypes_ptr(src), P, S, po, so, ctypes_ptr(dst)))
+            for _ in range(args.warmup):
+                call()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(st)
+            for _ in range(args.steps):
+                call()
+            e1.record(st)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / args.steps
+            got = dst.cpu().numpy().view(np.complex128)
+            t0 = time.perf_counter()
+            ref = RO.sk_resize(phs.real, (po, so)) + 1j * RO.sk_resize(phs.imag, (po, so))
+            cpu_s = time.perf_counter() - t0
+            rng_ = max(np.ptp(phs.real), np.ptp(phs.imag))
+            err = float(np.max(np.abs(got - ref)) / rng_)
+            nbytes = P * S * 16 + po * so * 16
+            cases.append({"case": name, "in": [P, S], "out": [po, so], "device_ms": ms,
+                          "roofline": {"bound": "hbm", "achieved": nbytes / (ms * 1e-3) / 1e9, "peak": hbm_peak,
+                                       "unit": "GB/s", "frac": nbytes / (ms * 1e-3) / 1e9 / hbm_peak,
+                                       "traffic": None, "algorithmic_bytes": nbytes},
+                          "cpu_ms": cpu_s * 1e3, "cpu_vs_device": cpu_s * 1e3 / ms,
+                          "max_abs_diff_over_range": err})
+    finally:
+        ctx.close()
+    res = {
+        "metric": "resize device time (ms), phase history 1999x1800 complex128 to twice its size",
+        "value": cases[0]["device_ms"], "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": cases[0]["device_ms"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded; the one-node Sandia run's phase-history shape)",
+        "config": {"workload": "resize: data/resize.py on a 1999x1800 complex128 phase history",
+                   "parallelism": "replicas1", "l2": "inputs and outputs > 126 MB L2 (up2), no flush"},
+        "cases": cases,
+        "cpu_baseline": {"kind": "port", "cores": 1, "unit": "ms",
+                         "sample": "the whole array, scipy.ndimage restatement of skimage's resize",
+                         "value": cases[0]["cpu_ms"]},
+    }
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+
+
+def ctypes_ptr(t):
+    import ctypes
+    return ctypes.c_void_p(t.data_ptr())
+
+
 def n_fft_of(S, u):
     return int(math.pow(2, int(math.log2(S * u)) + 1))  # sarbp.cpp:258
 
@@ -1171,6 +1258,8 @@ def main():
                 run_cli(args, rank, world, local_rank)
             elif args.config == "streamed":
                 run_streamed(args, rank, world, local_rank)
+            elif args.config == "resize":
+                run_resize(args, rank, world, local_rank)
             else:
                 run_ours(args, rank, world, local_rank)
     finally:

@@ -25,6 +25,7 @@
 // Arrays are [rows][cols][ncomp] of f32 or f64; each of the ncomp
 // interleaved components (re, im of a complex array) is resampled on its
 // own, as the reference does with np.real and np.imag.
+#include <algorithm>
 #include <cfloat>
 #include <cstdint>
 
@@ -38,6 +39,7 @@ namespace {
 constexpr int kThreads = 256;
 
 __device__ __forceinline__ long long mirror_index(long long m, long long n) {
+    if (m >= 0 && m < n) return m;  // inside: no reflection
     if (n <= 1) return 0;
     const long long period = 2 * n - 2;
     if (m < 0) m = -m;
@@ -45,26 +47,44 @@ __device__ __forceinline__ long long mirror_index(long long m, long long n) {
     return m >= n ? period - m : m;
 }
 
+// Launch shape of the per-element kernels: x over (column, component)
+// elements of a row, y over rows (strided; gridDim.y <= 65535), about 16
+// blocks per SM in all.
+struct RowGrid {
+    dim3 grid;
+};
+inline RowGrid row_grid(long long rows, long long row_elems) {
+    long long gx = (row_elems + kThreads - 1) / kThreads;
+    long long gy = rows;
+    const long long target = 148LL * 16;
+    if (gx >= target) gy = 1;
+    else gy = std::min<long long>(gy, std::max<long long>(1, target / gx));
+    gy = std::min<long long>(gy, 65535);
+    return RowGrid{dim3((unsigned)std::max<long long>(1, gx), (unsigned)std::max<long long>(1, gy))};
+}
+
 // One correlation pass along `axis` (0: rows, 1: cols) of [rows][cols][nc]
-// with symmetric weights w[0..r] (w[0] the centre).
+// with symmetric weights w[0..r] (w[0] the centre).  Thread: one (column,
+// component) element of a row, rows strided over y.
 template <typename T>
 __global__ void gauss_pass_kernel(const T *__restrict__ in, T *__restrict__ out, int rows, int cols, int nc,
                                   int axis, const double *__restrict__ w, int r) {
-    const long long n = (long long)rows * cols * nc;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(i % nc);
-        const long long rc = i / nc;
-        const int c = (int)(rc % cols), row = (int)(rc / cols);
-        const int pos = axis == 0 ? row : c, len = axis == 0 ? rows : cols;
-        auto at = [&](long long m) -> double {
-            const long long mm = mirror_index(m, len);
-            const long long idx = axis == 0 ? (mm * cols + c) * nc + k : ((long long)row * cols + mm) * nc + k;
-            return (double)in[idx];
-        };
-        double acc = at(pos) * w[0];
-        for (int j = r; j >= 1; --j) acc += (at((long long)pos - j) + at((long long)pos + j)) * w[j];
-        out[i] = (T)acc;
+    const long long row_elems = (long long)cols * nc;
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < row_elems;
+         j += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(j % nc);
+        const int c = (int)(j / nc);
+        for (int row = blockIdx.y; row < rows; row += gridDim.y) {
+            const int pos = axis == 0 ? row : c, len = axis == 0 ? rows : cols;
+            auto at = [&](long long m) -> double {
+                const long long mm = mirror_index(m, len);
+                const long long idx = axis == 0 ? (mm * cols + c) * nc + k : ((long long)row * cols + mm) * nc + k;
+                return (double)in[idx];
+            };
+            double acc = at(pos) * w[0];
+            for (int t = r; t >= 1; --t) acc += (at((long long)pos - t) + at((long long)pos + t)) * w[t];
+            out[(long long)row * row_elems + j] = (T)acc;
+        }
     }
 }
 
@@ -79,45 +99,101 @@ __device__ __forceinline__ double grid_coord(int o, double zoom, long long len) 
     return cc;
 }
 
+// The two neighbours (mirrored) and linear weights of output index o.
+struct Taps {
+    long long i0, i1;
+    double w0, w1;
+};
+__device__ __forceinline__ Taps taps_of(int o, double zoom, long long len) {
+    const double c = grid_coord(o, zoom, len);
+    const double f = floor(c);
+    const double t = c - f;
+    const long long a = (long long)f;
+    return Taps{mirror_index(a, len), mirror_index(a + 1, len), 1.0 - t, t};
+}
+
+// Thread: one (output column, component) element, its column taps formed
+// once, output rows strided over y; the four neighbours summed in f64 in
+// row-major order, each value times its row weight then its column weight.
 template <typename T>
 __global__ void zoom_kernel(const T *__restrict__ in, T *__restrict__ out, int rows, int cols, int nc,
                             int orows, int ocols, double z0, double z1, const double *__restrict__ bounds) {
-    const long long n = (long long)orows * ocols * nc;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(i % nc);
-        const long long rc = i / nc;
-        const int oc = (int)(rc % ocols), orow = (int)(rc / ocols);
-        const double c0 = grid_coord(orow, z0, rows), c1 = grid_coord(oc, z1, cols);
-        const double f0 = floor(c0), f1 = floor(c1);
-        const double t0 = c0 - f0, t1 = c1 - f1;
-        const double w0[2] = {1.0 - t0, t0}, w1[2] = {1.0 - t1, t1};
-        const long long a0 = (long long)f0, a1 = (long long)f1;
-        double t = 0.0;
-        for (int h0 = 0; h0 < 2; ++h0) {
-            const long long r0 = mirror_index(a0 + h0, rows);
-            for (int h1 = 0; h1 < 2; ++h1) {
-                const long long r1 = mirror_index(a1 + h1, cols);
-                double coeff = (double)in[(r0 * cols + r1) * nc + k];
-                coeff *= w0[h0];
-                coeff *= w1[h1];
-                t += coeff;
-            }
-        }
+    const long long row_elems = (long long)ocols * nc;
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < row_elems;
+         j += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(j % nc);
+        const Taps tc = taps_of((int)(j / nc), z1, cols);
         const double lo = bounds[2 * k], hi = bounds[2 * k + 1];
-        out[i] = (T)fmin(fmax(t, lo), hi);  // the bounds are values of type T
+        for (int orow = blockIdx.y; orow < orows; orow += gridDim.y) {
+            const Taps tr = taps_of(orow, z0, rows);
+            const long long r0 = tr.i0 * cols, r1 = tr.i1 * cols;
+            double t = 0.0, coeff;
+            coeff = (double)in[(r0 + tc.i0) * nc + k];
+            coeff *= tr.w0;
+            coeff *= tc.w0;
+            t += coeff;
+            coeff = (double)in[(r0 + tc.i1) * nc + k];
+            coeff *= tr.w0;
+            coeff *= tc.w1;
+            t += coeff;
+            coeff = (double)in[(r1 + tc.i0) * nc + k];
+            coeff *= tr.w1;
+            coeff *= tc.w0;
+            t += coeff;
+            coeff = (double)in[(r1 + tc.i1) * nc + k];
+            coeff *= tr.w1;
+            coeff *= tc.w1;
+            t += coeff;
+            out[(long long)orow * row_elems + j] = (T)fmin(fmax(t, lo), hi);  // the bounds are values of type T
+        }
     }
 }
 
-// [min, max] of each component (one block per component)
+// [min, max] of each component: partial bounds of kBoundBlocks slices of
+// the array (part[b][k] = (lo, hi)), then one block per component reduces
+// them (fmin / fmax: the order does not change the result)
+constexpr int kBoundBlocks = 148 * 4;
+
 template <typename T>
-__global__ void bounds_kernel(const T *__restrict__ in, long long count, int nc, double *__restrict__ bounds) {
+__global__ void __launch_bounds__(kThreads) bounds_partial_kernel(const T *__restrict__ in, long long count, int nc,
+                                                                  double *__restrict__ part) {
+    __shared__ double slo[kThreads / 32], shi[kThreads / 32];
+    for (int k = 0; k < nc; ++k) {
+        double lo = DBL_MAX, hi = -DBL_MAX;
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+             i += (long long)gridDim.x * blockDim.x) {
+            const double v = (double)in[i * nc + k];
+            lo = fmin(lo, v);
+            hi = fmax(hi, v);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            slo[threadIdx.x >> 5] = lo;
+            shi[threadIdx.x >> 5] = hi;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < kThreads / 32; ++w) {
+                lo = fmin(lo, slo[w]);
+                hi = fmax(hi, shi[w]);
+            }
+            part[((long long)blockIdx.x * nc + k) * 2] = lo;
+            part[((long long)blockIdx.x * nc + k) * 2 + 1] = hi;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) bounds_final_kernel(const double *__restrict__ part, int nparts, int nc,
+                                                                double *__restrict__ bounds) {
     const int k = blockIdx.x;
     double lo = DBL_MAX, hi = -DBL_MAX;
-    for (long long i = threadIdx.x; i < count; i += blockDim.x) {
-        const double v = (double)in[i * nc + k];
-        lo = fmin(lo, v);
-        hi = fmax(hi, v);
+    for (int b = threadIdx.x; b < nparts; b += blockDim.x) {
+        lo = fmin(lo, part[((long long)b * nc + k) * 2]);
+        hi = fmax(hi, part[((long long)b * nc + k) * 2 + 1]);
     }
     for (int o = 16; o > 0; o >>= 1) {
         lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
@@ -139,31 +215,27 @@ __global__ void bounds_kernel(const T *__restrict__ in, long long count, int nc,
     }
 }
 
-int grid_of(long long n) {
-    long long b = (n + kThreads - 1) / kThreads;
-    if (b > 148LL * 16) b = 148LL * 16;
-    return (int)(b < 1 ? 1 : b);
-}
-
 template <typename T>
 cudaError_t resize_t(const ResizePlan &p, const void *in, void *out, void *tmp_a, void *tmp_b, double *bounds,
                      cudaStream_t st) {
     const T *src = static_cast<const T *>(in);
     T *a = static_cast<T *>(tmp_a), *b = static_cast<T *>(tmp_b);
-    const long long n_in = (long long)p.rows * p.cols * p.nc;
-    bounds_kernel<T><<<p.nc, kThreads, 0, st>>>(src, (long long)p.rows * p.cols, p.nc, bounds);
+    // bounds[0 .. 2 nc) the result, bounds + 2 nc the partials
+    const long long count = (long long)p.rows * p.cols;
+    const int nparts = (int)std::min<long long>(kBoundBlocks, (count + kThreads - 1) / kThreads);
+    bounds_partial_kernel<T><<<nparts, kThreads, 0, st>>>(src, count, p.nc, bounds + 2 * p.nc);
+    bounds_final_kernel<<<p.nc, kThreads, 0, st>>>(bounds + 2 * p.nc, nparts, p.nc, bounds);
     // anti-aliasing passes, axis 0 then axis 1
     const T *cur = src;
     for (int axis = 0; axis < 2; ++axis) {
         if (p.radius[axis] < 0) continue;
         T *dst = (cur == a) ? b : a;
-        gauss_pass_kernel<T><<<grid_of(n_in), kThreads, 0, st>>>(cur, dst, p.rows, p.cols, p.nc, axis,
-                                                                 p.d_weights + p.woff[axis], p.radius[axis]);
+        gauss_pass_kernel<T><<<row_grid(p.rows, (long long)p.cols * p.nc).grid, kThreads, 0, st>>>(
+            cur, dst, p.rows, p.cols, p.nc, axis, p.d_weights + p.woff[axis], p.radius[axis]);
         cur = dst;
     }
-    const long long n_out = (long long)p.orows * p.ocols * p.nc;
-    zoom_kernel<T><<<grid_of(n_out), kThreads, 0, st>>>(cur, static_cast<T *>(out), p.rows, p.cols, p.nc, p.orows,
-                                                        p.ocols, p.zoom[0], p.zoom[1], bounds);
+    zoom_kernel<T><<<row_grid(p.orows, (long long)p.ocols * p.nc).grid, kThreads, 0, st>>>(
+        cur, static_cast<T *>(out), p.rows, p.cols, p.nc, p.orows, p.ocols, p.zoom[0], p.zoom[1], bounds);
     return cudaGetLastError();
 }
 
