@@ -78,6 +78,7 @@ struct ResizePlan {
     int radius[2];         // Gaussian radius per axis; -1: axis not filtered
     int woff[2];           // offset of each axis's weights w[0..radius] in d_weights
     const double *d_weights;
+    void *d_taps;          // (orows + ocols) * 32 bytes of scratch: the zoom's taps per index
 };
 cudaError_t launch_resize(const ResizePlan &p, const void *in, void *out, void *tmp_a, void *tmp_b,
                           double *bounds, cudaStream_t st);

@@ -48,15 +48,16 @@ __device__ __forceinline__ long long mirror_index(long long m, long long n) {
 }
 
 // Launch shape of the per-element kernels: x over (column, component)
-// elements of a row, y over rows (strided; gridDim.y <= 65535), about 16
-// blocks per SM in all.
+// elements of a row, y over rows (strided; gridDim.y <= 65535), up to 256
+// blocks per SM in all, so that each thread has only a few rows in turn
+// (its loads per row wait on memory; many warps hide that wait).
 struct RowGrid {
     dim3 grid;
 };
 inline RowGrid row_grid(long long rows, long long row_elems) {
     long long gx = (row_elems + kThreads - 1) / kThreads;
     long long gy = rows;
-    const long long target = 148LL * 16;
+    const long long target = 148LL * 256;
     if (gx >= target) gy = 1;
     else gy = std::min<long long>(gy, std::max<long long>(1, target / gx));
     gy = std::min<long long>(gy, 65535);
@@ -112,20 +113,29 @@ __device__ __forceinline__ Taps taps_of(int o, double zoom, long long len) {
     return Taps{mirror_index(a, len), mirror_index(a + 1, len), 1.0 - t, t};
 }
 
-// Thread: one (output column, component) element, its column taps formed
-// once, output rows strided over y; the four neighbours summed in f64 in
-// row-major order, each value times its row weight then its column weight.
+// taps[0 .. orows) of the output rows, taps[orows .. orows + ocols) of the
+// output columns
+__global__ void taps_kernel(Taps *__restrict__ taps, int orows, int ocols, double z0, double z1, int rows,
+                            int cols) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < orows) taps[i] = taps_of(i, z0, rows);
+    else if (i < orows + ocols) taps[i] = taps_of(i - orows, z1, cols);
+}
+
+// Thread: one (output column, component) element, output rows strided over
+// y; the four neighbours summed in f64 in row-major order, each value
+// times its row weight then its column weight.
 template <typename T>
 __global__ void zoom_kernel(const T *__restrict__ in, T *__restrict__ out, int rows, int cols, int nc,
-                            int orows, int ocols, double z0, double z1, const double *__restrict__ bounds) {
+                            int orows, int ocols, const Taps *__restrict__ taps, const double *__restrict__ bounds) {
     const long long row_elems = (long long)ocols * nc;
     for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < row_elems;
          j += (long long)gridDim.x * blockDim.x) {
         const int k = (int)(j % nc);
-        const Taps tc = taps_of((int)(j / nc), z1, cols);
+        const Taps tc = taps[orows + (int)(j / nc)];
         const double lo = bounds[2 * k], hi = bounds[2 * k + 1];
         for (int orow = blockIdx.y; orow < orows; orow += gridDim.y) {
-            const Taps tr = taps_of(orow, z0, rows);
+            const Taps tr = taps[orow];
             const long long r0 = tr.i0 * cols, r1 = tr.i1 * cols;
             double t = 0.0, coeff;
             coeff = (double)in[(r0 + tc.i0) * nc + k];
@@ -234,8 +244,12 @@ cudaError_t resize_t(const ResizePlan &p, const void *in, void *out, void *tmp_a
             cur, dst, p.rows, p.cols, p.nc, axis, p.d_weights + p.woff[axis], p.radius[axis]);
         cur = dst;
     }
+    Taps *taps = static_cast<Taps *>(p.d_taps);
+    const int ntaps = p.orows + p.ocols;
+    taps_kernel<<<(ntaps + kThreads - 1) / kThreads, kThreads, 0, st>>>(taps, p.orows, p.ocols, p.zoom[0],
+                                                                       p.zoom[1], p.rows, p.cols);
     zoom_kernel<T><<<row_grid(p.orows, (long long)p.ocols * p.nc).grid, kThreads, 0, st>>>(
-        cur, static_cast<T *>(out), p.rows, p.cols, p.nc, p.orows, p.ocols, p.zoom[0], p.zoom[1], bounds);
+        cur, static_cast<T *>(out), p.rows, p.cols, p.nc, p.orows, p.ocols, taps, bounds);
     return cudaGetLastError();
 }
 

@@ -88,7 +88,8 @@ int resize_enqueue(sarbp_ctx *ctx, int elem_bytes, int ncomp, const void *in, in
     // bounds: the result (2 ncomp) and the partials of up to 148 * 4 blocks
     const size_t b_w = a256(std::max<size_t>(1, weights.size()) * sizeof(double)),
                  b_b = a256((size_t)(1 + 148 * 4) * 2 * ncomp * sizeof(double));
-    cudaError_t e = ctx->resize_buf.ensure(b_w + b_b + 2 * a256(n_in), ctx->stream);
+    const size_t b_t = a256(((size_t)orows + ocols) * 32);
+    cudaError_t e = ctx->resize_buf.ensure(b_w + b_b + 2 * a256(n_in) + b_t, ctx->stream);
     if (e != cudaSuccess) return cuda_fail(e, "resize: scratch");
     char *base = static_cast<char *>(ctx->resize_buf.ptr);
     double *d_w = reinterpret_cast<double *>(base), *d_b = reinterpret_cast<double *>(base + b_w);
@@ -97,9 +98,10 @@ int resize_enqueue(sarbp_ctx *ctx, int elem_bytes, int ncomp, const void *in, in
                             ctx->stream);
     if (e != cudaSuccess) return cuda_fail(e, "resize: weights");
     p.d_weights = d_w;
+    p.d_taps = base + b_w + b_b + 2 * a256(n_in);
     e = launch_resize(p, in, out, base + b_w + b_b, base + b_w + b_b + a256(n_in), d_b, ctx->stream);
     if (e != cudaSuccess) return cuda_fail(e, "resize launch");
-    ctx->dev.launches += 3 + (p.radius[0] >= 0) + (p.radius[1] >= 0);
+    ctx->dev.launches += 4 + (p.radius[0] >= 0) + (p.radius[1] >= 0);
     return SARBP_OK;
 }
 
