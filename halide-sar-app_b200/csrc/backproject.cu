@@ -133,9 +133,10 @@ __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
 // One pulse (record rec, window at byte offset poff) for a consumer's pixel
 // pairs.  The sine and cosine are written straight into the pair registers
-// that the accumulation's f32x2 FMAs read.  PRE: the series products e^2
-// and e - e' come from the record's fourth float4 (formed by the producer)
-// instead of being formed per pulse here; the same f32 products either way.
+// that the accumulation's f32x2 FMAs read.  PRE: the series products (2 e^2
+// in mode 1, e^2 in mode 2, e - e') come from the record's fourth float4
+// (formed by the producer for the chunk's mode) instead of being formed per
+// pulse here; the same f32 products either way.
 // Kernels at 3 CTAs per SM take them from the record (0.9 % faster at
 // 2048^2 x 1999 by register assignment), those at 2 form them (batches of
 // uneven jobs, where the extra shared load cost as much as it saved).
@@ -151,18 +152,22 @@ __device__ __forceinline__ void pulse_step(const float4 *__restrict__ rec, uint3
     const float2 AX = f2(q0.x, q0.y), AY = f2(q0.z, q0.w), AZ = f2(q1.x, q1.y);
     const float2 E = f2(q1.z, q1.w), C0 = f2(q2.x, q2.y), B = f2(q2.z, q2.w);
     float Rp = 0.0f;
-    float2 EE = f2(0.0f), DE = f2(0.0f);
+    float2 EE = f2(0.0f), EE2 = f2(0.0f), DE = f2(0.0f);  // e^2, 2 e^2, e - e'
     if constexpr (PRE) {
         if constexpr (MODE >= 1) {
-            const float4 q3 = rec[3];  // (e^2, e^2, e - e', e - e'), or (k_c R, 0, ...) in mode 3
+            // (2 e^2, 2 e^2, e - e', e - e') in mode 1, (e^2, e^2, ...) in
+            // mode 2, (k_c R, 0, ...) in mode 3
+            const float4 q3 = rec[3];
             DE = f2(q3.z, q3.w);
             if constexpr (MODE == 3) Rp = q3.x;
+            else if constexpr (MODE == 1) EE2 = f2(q3.x, q3.y);
             else EE = f2(q3.x, q3.y);
         }
     } else {
         if constexpr (MODE == 3) Rp = rec[3].x;
         const float ee = q1.z * q1.z;
         EE = f2(ee);
+        EE2 = __fadd2_rn(EE, EE);
         const float de = -4.0f * ee * q2.z;  // e - e' (narrow tiles)
         DE = f2(de);
     }
@@ -183,11 +188,11 @@ __device__ __forceinline__ void pulse_step(const float4 *__restrict__ rec, uint3
             s = __fadd2_rn(s0[j], sd);
             // mode 1 folds its third series term into the second:
             // e t + 2 e^2 s t = (e + 2 e^2 s) t
-            const float2 Et = MODE == 1 ? __ffma2_rn(__fadd2_rn(EE, EE), s, E) : E;
+            const float2 Et = MODE == 1 ? __ffma2_rn(EE2, s, E) : E;
             D = __fadd2_rn(__ffma2_rn(Et, __ffma2_rn(s, s, nd2[j]), sd), B);
         }
         if constexpr (MODE == 1 && !WIDE) {
-            D = __ffma2_rn(__fmul2_rn(__fadd2_rn(EE, EE), s), __ffma2_rn(s, s, nd2[j]), D);
+            D = __ffma2_rn(__fmul2_rn(EE2, s), __ffma2_rn(s, s, nd2[j]), D);
         } else if constexpr (MODE == 2) {
             const float2 h = __ffma2_rn(E, nd2[j], s);
             const float2 q = __ffma2_rn(__fmul2_rn(f2(5.0f), E), h, f2(2.0f));
@@ -332,8 +337,9 @@ __device__ __forceinline__ bool stage_chunk(const DevJob &jb, int tile, int lane
         mode = max(mode, __shfl_xor_sync(0xffffffffu, mode, o));
     }
     // records as the consumers read them: four float4 of broadcast pairs;
-    // the fourth holds the per-pulse products of the series terms (e^2 and
-    // e - e' = -4 e^2 sigma0), or k_c R for the closed form (mode 3)
+    // the fourth holds the per-pulse products of the series terms the
+    // chunk's mode uses (2 e^2 in mode 1, e^2 in mode 2, and e - e' =
+    // -4 e^2 sigma0), or k_c R for the closed form (mode 3)
     float4 *r2 = sm.rec2 + (size_t)b * 4 * cmax;
     for (int i = lane; i < nc; i += 32) {
         const float4 a = rec[i].a, q = rec[i].b;
@@ -342,7 +348,8 @@ __device__ __forceinline__ bool stage_chunk(const DevJob &jb, int tile, int lane
         r2[4 * i + 2] = make_float4(q.x, q.x, q.y, q.y);
         const float ee = a.w * a.w;
         const float de = -4.0f * ee * q.y;
-        r2[4 * i + 3] = mode == 3 ? make_float4(q.z, 0.0f, de, de) : make_float4(ee, ee, de, de);
+        const float e2 = mode == 1 ? ee + ee : ee;
+        r2[4 * i + 3] = mode == 3 ? make_float4(q.z, 0.0f, de, de) : make_float4(e2, e2, de, de);
     }
     if (lane == 0) {
         sm.s_mode[b] = mode;
