@@ -47,44 +47,55 @@ __device__ __forceinline__ long long mirror_index(long long m, long long n) {
     return m >= n ? period - m : m;
 }
 
-// Launch shape of the per-element kernels: x over (column, component)
-// elements of a row, y over rows (strided; gridDim.y <= 65535), up to 256
-// blocks per SM in all, so that each thread has only a few rows in turn
-// (its loads per row wait on memory; many warps hide that wait).
+// Launch shape of the per-column kernels: x over the columns of a row, y
+// over rows (strided; gridDim.y <= 65535), about 32 blocks per SM in all.
 struct RowGrid {
     dim3 grid;
 };
-inline RowGrid row_grid(long long rows, long long row_elems) {
-    long long gx = (row_elems + kThreads - 1) / kThreads;
+inline RowGrid row_grid(long long rows, long long cols) {
+    long long gx = (cols + kThreads - 1) / kThreads;
     long long gy = rows;
-    const long long target = 148LL * 256;
+    const long long target = 148LL * 32;
     if (gx >= target) gy = 1;
     else gy = std::min<long long>(gy, std::max<long long>(1, target / gx));
     gy = std::min<long long>(gy, 65535);
     return RowGrid{dim3((unsigned)std::max<long long>(1, gx), (unsigned)std::max<long long>(1, gy))};
 }
 
+// Components per element: NC > 0 fixed at compile time (1, or 2 for the
+// real and imaginary parts of a complex array), NC == 0 taken from nc.
+template <int NC>
+__device__ __forceinline__ int ncomp(int nc) {
+    return NC > 0 ? NC : nc;
+}
+
 // One correlation pass along `axis` (0: rows, 1: cols) of [rows][cols][nc]
-// with symmetric weights w[0..r] (w[0] the centre).  Thread: one (column,
-// component) element of a row, rows strided over y.
-template <typename T>
-__global__ void gauss_pass_kernel(const T *__restrict__ in, T *__restrict__ out, int rows, int cols, int nc,
+// with symmetric weights w[0..r] (w[0] the centre).  Thread: one column of
+// a row (all its components), rows strided over y.
+template <typename T, int NC>
+__global__ void gauss_pass_kernel(const T *__restrict__ in, T *__restrict__ out, int rows, int cols, int nc_,
                                   int axis, const double *__restrict__ w, int r) {
-    const long long row_elems = (long long)cols * nc;
-    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < row_elems;
-         j += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(j % nc);
-        const int c = (int)(j / nc);
+    const int nc = ncomp<NC>(nc_);
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x) {
         for (int row = blockIdx.y; row < rows; row += gridDim.y) {
             const int pos = axis == 0 ? row : c, len = axis == 0 ? rows : cols;
-            auto at = [&](long long m) -> double {
+            // first value of the element at position m along the axis
+            auto base = [&](long long m) -> long long {
                 const long long mm = mirror_index(m, len);
-                const long long idx = axis == 0 ? (mm * cols + c) * nc + k : ((long long)row * cols + mm) * nc + k;
-                return (double)in[idx];
+                return (axis == 0 ? mm * cols + c : (long long)row * cols + mm) * nc;
             };
-            double acc = at(pos) * w[0];
-            for (int t = r; t >= 1; --t) acc += (at((long long)pos - t) + at((long long)pos + t)) * w[t];
-            out[(long long)row * row_elems + j] = (T)acc;
+            const long long b0 = base(pos);
+            T *o = out + ((long long)row * cols + c) * nc;
+#pragma unroll
+            for (int k = 0; k < (NC > 0 ? NC : 1); ++k) {
+                for (int kk = k; kk < nc; kk += (NC > 0 ? NC : 1)) {
+                    double acc = (double)in[b0 + kk] * w[0];
+                    for (int t = r; t >= 1; --t)
+                        acc += ((double)in[base((long long)pos - t) + kk] + (double)in[base((long long)pos + t) + kk]) *
+                               w[t];
+                    o[kk] = (T)acc;
+                }
+            }
         }
     }
 }
@@ -122,39 +133,43 @@ __global__ void taps_kernel(Taps *__restrict__ taps, int orows, int ocols, doubl
     else if (i < orows + ocols) taps[i] = taps_of(i - orows, z1, cols);
 }
 
-// Thread: one (output column, component) element, output rows strided over
-// y; the four neighbours summed in f64 in row-major order, each value
+// Thread: one output column (all its components), output rows strided
+// over y; the four neighbours summed in f64 in row-major order, each value
 // times its row weight then its column weight.
-template <typename T>
-__global__ void zoom_kernel(const T *__restrict__ in, T *__restrict__ out, int rows, int cols, int nc,
+template <typename T, int NC>
+__global__ void zoom_kernel(const T *__restrict__ in, T *__restrict__ out, int rows, int cols, int nc_,
                             int orows, int ocols, const Taps *__restrict__ taps, const double *__restrict__ bounds) {
-    const long long row_elems = (long long)ocols * nc;
-    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < row_elems;
-         j += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(j % nc);
-        const Taps tc = taps[orows + (int)(j / nc)];
-        const double lo = bounds[2 * k], hi = bounds[2 * k + 1];
+    const int nc = ncomp<NC>(nc_);
+    for (int oc = blockIdx.x * blockDim.x + threadIdx.x; oc < ocols; oc += gridDim.x * blockDim.x) {
+        const Taps tc = taps[orows + oc];
         for (int orow = blockIdx.y; orow < orows; orow += gridDim.y) {
             const Taps tr = taps[orow];
-            const long long r0 = tr.i0 * cols, r1 = tr.i1 * cols;
-            double t = 0.0, coeff;
-            coeff = (double)in[(r0 + tc.i0) * nc + k];
-            coeff *= tr.w0;
-            coeff *= tc.w0;
-            t += coeff;
-            coeff = (double)in[(r0 + tc.i1) * nc + k];
-            coeff *= tr.w0;
-            coeff *= tc.w1;
-            t += coeff;
-            coeff = (double)in[(r1 + tc.i0) * nc + k];
-            coeff *= tr.w1;
-            coeff *= tc.w0;
-            t += coeff;
-            coeff = (double)in[(r1 + tc.i1) * nc + k];
-            coeff *= tr.w1;
-            coeff *= tc.w1;
-            t += coeff;
-            out[(long long)orow * row_elems + j] = (T)fmin(fmax(t, lo), hi);  // the bounds are values of type T
+            const T *p00 = in + (tr.i0 * cols + tc.i0) * nc, *p01 = in + (tr.i0 * cols + tc.i1) * nc;
+            const T *p10 = in + (tr.i1 * cols + tc.i0) * nc, *p11 = in + (tr.i1 * cols + tc.i1) * nc;
+            T *o = out + ((long long)orow * ocols + oc) * nc;
+#pragma unroll
+            for (int k = 0; k < (NC > 0 ? NC : 1); ++k) {
+                for (int kk = k; kk < nc; kk += (NC > 0 ? NC : 1)) {
+                    double t = 0.0, coeff;
+                    coeff = (double)p00[kk];
+                    coeff *= tr.w0;
+                    coeff *= tc.w0;
+                    t += coeff;
+                    coeff = (double)p01[kk];
+                    coeff *= tr.w0;
+                    coeff *= tc.w1;
+                    t += coeff;
+                    coeff = (double)p10[kk];
+                    coeff *= tr.w1;
+                    coeff *= tc.w0;
+                    t += coeff;
+                    coeff = (double)p11[kk];
+                    coeff *= tr.w1;
+                    coeff *= tc.w1;
+                    t += coeff;
+                    o[kk] = (T)fmin(fmax(t, bounds[2 * kk]), bounds[2 * kk + 1]);  // the bounds are values of type T
+                }
+            }
         }
     }
 }
@@ -240,16 +255,28 @@ cudaError_t resize_t(const ResizePlan &p, const void *in, void *out, void *tmp_a
     for (int axis = 0; axis < 2; ++axis) {
         if (p.radius[axis] < 0) continue;
         T *dst = (cur == a) ? b : a;
-        gauss_pass_kernel<T><<<row_grid(p.rows, (long long)p.cols * p.nc).grid, kThreads, 0, st>>>(
-            cur, dst, p.rows, p.cols, p.nc, axis, p.d_weights + p.woff[axis], p.radius[axis]);
+        const dim3 g = row_grid(p.rows, p.cols).grid;
+        const double *w = p.d_weights + p.woff[axis];
+        if (p.nc == 1)
+            gauss_pass_kernel<T, 1><<<g, kThreads, 0, st>>>(cur, dst, p.rows, p.cols, 1, axis, w, p.radius[axis]);
+        else if (p.nc == 2)
+            gauss_pass_kernel<T, 2><<<g, kThreads, 0, st>>>(cur, dst, p.rows, p.cols, 2, axis, w, p.radius[axis]);
+        else
+            gauss_pass_kernel<T, 0><<<g, kThreads, 0, st>>>(cur, dst, p.rows, p.cols, p.nc, axis, w, p.radius[axis]);
         cur = dst;
     }
     Taps *taps = static_cast<Taps *>(p.d_taps);
     const int ntaps = p.orows + p.ocols;
     taps_kernel<<<(ntaps + kThreads - 1) / kThreads, kThreads, 0, st>>>(taps, p.orows, p.ocols, p.zoom[0],
                                                                        p.zoom[1], p.rows, p.cols);
-    zoom_kernel<T><<<row_grid(p.orows, (long long)p.ocols * p.nc).grid, kThreads, 0, st>>>(
-        cur, static_cast<T *>(out), p.rows, p.cols, p.nc, p.orows, p.ocols, taps, bounds);
+    const dim3 g = row_grid(p.orows, p.ocols).grid;
+    T *o = static_cast<T *>(out);
+    if (p.nc == 1)
+        zoom_kernel<T, 1><<<g, kThreads, 0, st>>>(cur, o, p.rows, p.cols, 1, p.orows, p.ocols, taps, bounds);
+    else if (p.nc == 2)
+        zoom_kernel<T, 2><<<g, kThreads, 0, st>>>(cur, o, p.rows, p.cols, 2, p.orows, p.ocols, taps, bounds);
+    else
+        zoom_kernel<T, 0><<<g, kThreads, 0, st>>>(cur, o, p.rows, p.cols, p.nc, p.orows, p.ocols, taps, bounds);
     return cudaGetLastError();
 }
 
