@@ -86,9 +86,23 @@ __global__ void gauss_pass_kernel(const T *__restrict__ in, T *__restrict__ out,
             };
             const long long b0 = base(pos);
             T *o = out + ((long long)row * cols + c) * nc;
+            if constexpr (NC > 0) {
+                // the components side by side, the taps unrolled, so that
+                // the loads of several taps are in flight together
+                double acc[NC];
 #pragma unroll
-            for (int k = 0; k < (NC > 0 ? NC : 1); ++k) {
-                for (int kk = k; kk < nc; kk += (NC > 0 ? NC : 1)) {
+                for (int k = 0; k < NC; ++k) acc[k] = (double)in[b0 + k] * w[0];
+#pragma unroll 4
+                for (int t = r; t >= 1; --t) {
+                    const long long bm = base((long long)pos - t), bp = base((long long)pos + t);
+                    const double wt = w[t];
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) acc[k] += ((double)in[bm + k] + (double)in[bp + k]) * wt;
+                }
+#pragma unroll
+                for (int k = 0; k < NC; ++k) o[k] = (T)acc[k];
+            } else {
+                for (int kk = 0; kk < nc; ++kk) {
                     double acc = (double)in[b0 + kk] * w[0];
                     for (int t = r; t >= 1; --t)
                         acc += ((double)in[base((long long)pos - t) + kk] + (double)in[base((long long)pos + t) + kk]) *
@@ -142,6 +156,7 @@ __global__ void zoom_kernel(const T *__restrict__ in, T *__restrict__ out, int r
     const int nc = ncomp<NC>(nc_);
     for (int oc = blockIdx.x * blockDim.x + threadIdx.x; oc < ocols; oc += gridDim.x * blockDim.x) {
         const Taps tc = taps[orows + oc];
+#pragma unroll 4
         for (int orow = blockIdx.y; orow < orows; orow += gridDim.y) {
             const Taps tr = taps[orow];
             const T *p00 = in + (tr.i0 * cols + tc.i0) * nc, *p01 = in + (tr.i0 * cols + tc.i1) * nc;
