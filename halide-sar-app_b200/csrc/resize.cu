@@ -194,34 +194,52 @@ __global__ void zoom_kernel(const T *__restrict__ in, T *__restrict__ out, int r
 // them (fmin / fmax: the order does not change the result)
 constexpr int kBoundBlocks = 148 * 4;
 
-template <typename T>
-__global__ void __launch_bounds__(kThreads) bounds_partial_kernel(const T *__restrict__ in, long long count, int nc,
+template <typename T, int NC>
+__global__ void __launch_bounds__(kThreads) bounds_partial_kernel(const T *__restrict__ in, long long count, int nc_,
                                                                   double *__restrict__ part) {
-    __shared__ double slo[kThreads / 32], shi[kThreads / 32];
-    for (int k = 0; k < nc; ++k) {
-        double lo = DBL_MAX, hi = -DBL_MAX;
+    // NC > 0: the NC components in one sweep; NC == 0: one sweep per component
+    constexpr int KB = NC > 0 ? NC : 1;
+    const int nc = NC > 0 ? NC : nc_;
+    __shared__ double slo[KB][kThreads / 32], shi[KB][kThreads / 32];
+    for (int k0 = 0; k0 < nc; k0 += KB) {
+        double lo[KB], hi[KB];
+#pragma unroll
+        for (int k = 0; k < KB; ++k) {
+            lo[k] = DBL_MAX;
+            hi[k] = -DBL_MAX;
+        }
         for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
              i += (long long)gridDim.x * blockDim.x) {
-            const double v = (double)in[i * nc + k];
-            lo = fmin(lo, v);
-            hi = fmax(hi, v);
+#pragma unroll
+            for (int k = 0; k < KB; ++k) {
+                const double v = (double)in[i * nc + k0 + k];
+                lo[k] = fmin(lo[k], v);
+                hi[k] = fmax(hi[k], v);
+            }
         }
-        for (int o = 16; o > 0; o >>= 1) {
-            lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-            hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-        }
-        if ((threadIdx.x & 31) == 0) {
-            slo[threadIdx.x >> 5] = lo;
-            shi[threadIdx.x >> 5] = hi;
+#pragma unroll
+        for (int k = 0; k < KB; ++k) {
+            for (int o = 16; o > 0; o >>= 1) {
+                lo[k] = fmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+                hi[k] = fmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+            }
+            if ((threadIdx.x & 31) == 0) {
+                slo[k][threadIdx.x >> 5] = lo[k];
+                shi[k][threadIdx.x >> 5] = hi[k];
+            }
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            for (int w = 1; w < kThreads / 32; ++w) {
-                lo = fmin(lo, slo[w]);
-                hi = fmax(hi, shi[w]);
+#pragma unroll
+            for (int k = 0; k < KB; ++k) {
+                double l = slo[k][0], h = shi[k][0];
+                for (int w = 1; w < kThreads / 32; ++w) {
+                    l = fmin(l, slo[k][w]);
+                    h = fmax(h, shi[k][w]);
+                }
+                part[((long long)blockIdx.x * nc + k0 + k) * 2] = l;
+                part[((long long)blockIdx.x * nc + k0 + k) * 2 + 1] = h;
             }
-            part[((long long)blockIdx.x * nc + k) * 2] = lo;
-            part[((long long)blockIdx.x * nc + k) * 2 + 1] = hi;
         }
         __syncthreads();
     }
@@ -263,7 +281,12 @@ cudaError_t resize_t(const ResizePlan &p, const void *in, void *out, void *tmp_a
     // bounds[0 .. 2 nc) the result, bounds + 2 nc the partials
     const long long count = (long long)p.rows * p.cols;
     const int nparts = (int)std::min<long long>(kBoundBlocks, (count + kThreads - 1) / kThreads);
-    bounds_partial_kernel<T><<<nparts, kThreads, 0, st>>>(src, count, p.nc, bounds + 2 * p.nc);
+    if (p.nc == 1)
+        bounds_partial_kernel<T, 1><<<nparts, kThreads, 0, st>>>(src, count, 1, bounds + 2);
+    else if (p.nc == 2)
+        bounds_partial_kernel<T, 2><<<nparts, kThreads, 0, st>>>(src, count, 2, bounds + 4);
+    else
+        bounds_partial_kernel<T, 0><<<nparts, kThreads, 0, st>>>(src, count, p.nc, bounds + 2 * p.nc);
     bounds_final_kernel<<<p.nc, kThreads, 0, st>>>(bounds + 2 * p.nc, nparts, p.nc, bounds);
     // anti-aliasing passes, axis 0 then axis 1
     const T *cur = src;
