@@ -1,6 +1,7 @@
 // geometry.cu -- f64 geometry of the pixel tiles, ahead of the FP32 loop.
 //
-// tile_setup_kernel (one CTA per (job, tile)) forms the tile's geometry and
+// tile_setup_kernel (one CTA per (job, tile), whatever the pulse parts of the
+// backprojection's work items) forms the tile's geometry and
 // then its pulse records:
 //   rc    = centre of the bounding box of the tile's pixel positions
 //   wide  = k_c * rho > kWideRad (rho below); then w0 = unit

@@ -181,8 +181,10 @@ int sarbp_range_compress_device(sarbp_ctx *ctx, const sarbp_job *job,
 /*
  * Many jobs of uneven size in one batch: one window kernel, one range
  * compression launch per distinct N_fft, and one persistent backprojection
- * launch over a (job, pixel tile) work list ordered longest-first.
- * Enqueued on the context's stream, not synchronised.
+ * launch over a (job, pixel tile, pulse part) work list ordered
+ * longest-first (small jobs split their tiles' pulses into parts, see
+ * sarbp_opts.pulse_parts), then one combine launch for the jobs formed in
+ * parts.  Enqueued on the context's stream, not synchronised.
  */
 int sarbp_batch_device(sarbp_ctx *ctx, const sarbp_job *jobs, int njobs,
                        const sarbp_opts *opts);
