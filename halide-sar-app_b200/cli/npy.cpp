@@ -1,10 +1,15 @@
 // npy.cpp -- .npy reader/writer (see npy.h).
 #include "npy.h"
 
+#include <unistd.h>
+
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
+#include <thread>
+#include <vector>
 
 namespace sarbp_cli {
 
@@ -17,6 +22,30 @@ using File = std::unique_ptr<FILE, FileCloser>;
 
 [[noreturn]] void bad(const std::string &path, const std::string &what) {
     throw std::runtime_error("npy: " + path + ": " + what);
+}
+
+// n bytes of fd from offset off into dst; payloads of many megabytes (the
+// phase history) in pieces on several threads; false on a short read
+bool read_at(int fd, off_t off, unsigned char *dst, size_t n) {
+    const size_t min_piece = 8u << 20;
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t parts = std::max<size_t>(1, std::min<size_t>(std::min<size_t>(hw, 8), n / min_piece));
+    std::vector<char> ok(parts, 0);
+    auto piece = [&](size_t i) {
+        size_t a = n * i / parts;
+        const size_t b = n * (i + 1) / parts;
+        while (a < b) {
+            const ssize_t r = pread(fd, dst + a, b - a, off + (off_t)a);
+            if (r <= 0) return;
+            a += (size_t)r;
+        }
+        ok[i] = 1;
+    };
+    std::vector<std::thread> th;
+    for (size_t i = 1; i < parts; ++i) th.emplace_back(piece, i);
+    piece(0);
+    for (auto &t : th) t.join();
+    return std::all_of(ok.begin(), ok.end(), [](char c) { return c != 0; });
 }
 
 // value text that follows 'key': in the header dict, trimmed at the next
@@ -101,8 +130,9 @@ NpyArray npy_load(const std::string &path) {
     }
 
     const size_t n = a.num_vals() * a.word_size;
-    a.bytes.resize(n);
-    if (n && std::fread(a.bytes.data(), 1, n, f.get()) != n) bad(path, "truncated data");
+    a.bytes.reset(new unsigned char[n ? n : 1]);
+    const long pos = std::ftell(f.get());
+    if (n && (pos < 0 || !read_at(fileno(f.get()), (off_t)pos, a.bytes.get(), n))) bad(path, "truncated data");
     return a;
 }
 

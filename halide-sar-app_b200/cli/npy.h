@@ -8,6 +8,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -18,7 +19,8 @@ struct NpyArray {
     size_t word_size = 0;         // bytes per element
     bool fortran_order = false;
     std::vector<size_t> shape;
-    std::vector<unsigned char> bytes;  // num_vals() * word_size
+    // num_vals() * word_size bytes of payload (not zero-filled before the read)
+    std::unique_ptr<unsigned char[]> bytes;
 
     size_t num_vals() const {
         size_t n = 1;
@@ -26,7 +28,7 @@ struct NpyArray {
         return n;
     }
     template <class T>
-    const T *data() const { return reinterpret_cast<const T *>(bytes.data()); }
+    const T *data() const { return reinterpret_cast<const T *>(bytes.get()); }
 };
 
 // Throws std::runtime_error with the file name on malformed input.

@@ -2,15 +2,34 @@
 // platform_data.h for the files and the error behaviour.
 #include "platform_data.h"
 
+#include <algorithm>
 #include <cstdio>
 #include <iostream>
 #include <stdexcept>
+#include <thread>
+#include <vector>
 
 #include "npy.h"
 
 namespace sarbp_cli {
 
 namespace {
+
+// out[i] = (float)in[i]; large arrays (the phase history) on several
+// threads, each converting one contiguous piece
+void downcast(const double *in, float *out, size_t n) {
+    const size_t min_piece = 1u << 20;
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t parts = std::max<size_t>(1, std::min<size_t>(std::min<size_t>(hw, 16), n / min_piece));
+    auto piece = [&](size_t i) {
+        const size_t a = n * i / parts, b = n * (i + 1) / parts;
+        for (size_t k = a; k < b; ++k) out[k] = (float)in[k];
+    };
+    std::vector<std::thread> th;
+    for (size_t i = 1; i < parts; ++i) th.emplace_back(piece, i);
+    piece(0);
+    for (auto &t : th) t.join();
+}
 
 bool file_exists(const std::string &path) {
     if (FILE *f = std::fopen(path.c_str(), "rb")) {
@@ -55,8 +74,7 @@ public:
             std::copy(s, s + out.size(), out.begin());
         } else if (a.word_size == sizeof(double)) {
             std::cout << "PlatformData: downcasting " << name << " from double to float" << std::endl;
-            const double *s = a.data<double>();
-            for (size_t i = 0; i < out.size(); ++i) out[i] = (float)s[i];
+            downcast(a.data<double>(), out.data(), out.size());
         } else {
             bad_word(name);
         }
@@ -92,8 +110,7 @@ public:
         } else if (a.word_size == 2 * sizeof(double)) {
             std::cout << "PlatformData: downcasting " << name
                       << " from complex<double> to complex<float>" << std::endl;
-            const double *s = a.data<double>();
-            for (size_t i = 0; i < out.size(); ++i) out[i] = (float)s[i];
+            downcast(a.data<double>(), out.data(), out.size());
         } else {
             bad_word(name);
         }
