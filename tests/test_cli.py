@@ -128,3 +128,16 @@ def test_halide_shim_refuses_bad_buffers():
     assert L.img_output_to_dB(img.ptr(), wrong_type.ptr()) < 0
     img.buf.flags = 2                                 # device_dirty
     assert L.img_output_to_dB(img.ptr(), HalideBuffer(np.zeros((4, 4))).ptr()) < 0
+
+
+def test_loader_rejects_a_truncated_payload(cli_built, tmp_path, afrl_input):
+    """A phase history whose payload ends early (the threaded read of the
+    payload in pieces) is an error naming the file, not a partial array."""
+    d = write_platform(str(tmp_path / "cut"), afrl_input, wide=True)
+    path = os.path.join(d, "phs.npy")
+    size = os.path.getsize(path)
+    with open(path, "r+b") as f:
+        f.truncate(size - 12345)
+    rc, out, err = _run("-p", d, "-o", str(tmp_path / "o.png"), "-d", "-30")
+    assert rc != 0 and "phs.npy" in err and "truncated data" in err, (out, err)
+    assert "Loaded platform data" not in out
