@@ -23,8 +23,9 @@ form), --config serve (the serving sweep), --config cli_sandia (the sarbp
 CLI end to end with the reference's one-node Sandia command line, beside the
 stage times of that run's log), --config streamed (a 4096^2 x 4000 image
 formed in pulse chunks under a device-memory cap), --config resize (the
-data/resize.py resampling on the device beside its scipy restatement), and
-any synth configuration name.
+data/resize.py resampling on the device beside its scipy restatement),
+--config distributed (the row-block schedule with its NCCL gather), and any
+synth configuration name.
 
 --impl reference times the reference algorithm's CPU implementation (the
 C restatement in oracle/, reference precision, all host threads) on a
@@ -1218,6 +1219,84 @@ def run_resize(args, rank, world, local_rank):
         print(json.dumps(res), flush=True)
 
 
+def run_distributed(args, rank, world, local_rank):
+    """--config distributed: the reference's -s cuda_distributed schedule
+    (backprojection.cpp:239-243) on plain_large through
+    sarbp_b200.distributed: each rank forms its block of output rows into a
+    device send buffer, NCCL gathers the blocks on rank 0, which copies the
+    image to the host once.  One image per step, timed on the host clock
+    between barriers (the call ends with rank 0's host copy), max over
+    ranks; under torchrun each of N ranks forms nv / N rows (strong
+    scaling); without it a one-rank NCCL group.  Rank 0's image is checked
+    against the plain device call of the same job (bit for bit at N = 1)."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    import sarbp_b200 as sb
+    from sarbp_b200 import synth
+    from sarbp_b200.distributed import DeviceCompute, distributed_backprojection
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    own_group = not dist.is_initialized()
+    if own_group:
+        import socket
+        with socket.socket() as so:
+            so.bind(("127.0.0.1", 0))
+            port = so.getsockname()[1]
+        dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=0, world_size=1,
+                                timeout=datetime.timedelta(seconds=120), device_id=dev)
+    try:
+        d = synth.make("plain_large", seed=2, with_r=False)
+        nu, nv, P = d["nu"], d["nv"], d["P"]
+        ctx = sb.Context(local_rank)
+        k32, p32 = d["k_r"].astype(np.float32), d["pos"].astype(np.float32)
+        comp = DeviceCompute(ctx, d["phs"], k32, d["taylor"], d["N_fft"], d["delta_r"], d["u"], d["v"], p32,
+                             u_hat=d["u_hat"], v_hat=d["v_hat"])
+        # rank 0's image lands in page-locked host memory, allocated once
+        out = torch.empty((nv, nu, 2), dtype=torch.float64).pin_memory().numpy().view(np.complex128)[..., 0] \
+            if rank == 0 else None
+        img = None
+        for _ in range(args.warmup):
+            img = distributed_backprojection(comp, nu, nv, out=out)
+        ts = []
+        for _ in range(args.steps):
+            dist.barrier(device_ids=[local_rank])
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            img = distributed_backprojection(comp, nu, nv, out=out)
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        t = torch.tensor([statistics.median(ts)], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sec = float(t.item())
+        same = None
+        if rank == 0:
+            ref = ctx.backprojection_plane(d["phs"], k32, d["taylor"], d["N_fft"], d["delta_r"], d["u"], d["v"],
+                                           d["u_hat"], d["v_hat"], p32)
+            same = bool(np.array_equal(img, ref)) if dist.get_world_size() == 1 else \
+                float(np.linalg.norm(img - ref) / np.linalg.norm(ref))
+        ctx.close()
+        n = dist.get_world_size()
+        if rank == 0:
+            units = float(nu) * nv * P
+            print(json.dumps({
+                "metric": "Gpixel*pulses/s (2048^2 x 1999, distributed row blocks gathered to rank 0)",
+                "value": units / sec / 1e9, "unit": "Gpixel*pulses/s", "n_gpus": n, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f32 (split-precision; f64 per-pulse set-up)",
+                "data": "synthetic (seeded, plain_large shapes)",
+                "config": {"workload": "distributed: plain_large, %d output-row block(s), NCCL gather to rank 0, "
+                                       "one host copy of the image" % n, "parallelism": "rows%d" % n,
+                           "l2": "inputs+outputs > 126 MB L2, no flush"},
+                "timing": "host clock between barriers, median of steps, max over ranks",
+                "image_vs_plain_call": same,
+            }), flush=True)
+    finally:
+        if own_group:
+            dist.destroy_process_group()
+
+
 def ctypes_ptr(t):
     import ctypes
     return ctypes.c_void_p(t.data_ptr())
@@ -1260,6 +1339,8 @@ def main():
                 run_streamed(args, rank, world, local_rank)
             elif args.config == "resize":
                 run_resize(args, rank, world, local_rank)
+            elif args.config == "distributed":
+                run_distributed(args, rank, world, local_rank)
             else:
                 run_ours(args, rank, world, local_rank)
     finally:

@@ -95,22 +95,30 @@ def form_block(compute, nu, nv, world, rank, device="cpu"):
     return send
 
 
-def assemble(gathered, nu, nv):
+def assemble(gathered, nu, nv, out=None):
     """The image complex128 [nv, nu] (host) from the ranks' send buffers in
-    rank order: the blocks are joined where they lie, then copied once."""
+    rank order, each block copied once into its rows of `out` (a C-order
+    complex128 [nv, nu] host array, written in place; page-locked memory
+    makes the device-to-host copies fastest) or of a new array."""
     import torch
     world = len(gathered)
-    parts = [g[: y1 - y0] for g, (y0, y1) in zip(gathered, output_row_blocks(nv, world)) if y1 > y0]
-    full = torch.cat(parts, 0)
-    return np.ascontiguousarray(full.cpu().numpy()).view(np.complex128)[..., 0]
+    if out is None:
+        out = np.empty((nv, nu), np.complex128)
+    if out.shape != (nv, nu) or out.dtype != np.complex128 or not out.flags.c_contiguous:
+        raise ValueError("out must be a C-order complex128 [nv, nu] array")
+    o = torch.from_numpy(out.view(np.float64).reshape(nv, nu, 2))
+    for g, (y0, y1) in zip(gathered, output_row_blocks(nv, world)):
+        if y1 > y0:
+            o[y0:y1].copy_(g[: y1 - y0])
+    return out
 
 
-def distributed_backprojection(compute, nu, nv, group=None, dst=0):
+def distributed_backprojection(compute, nu, nv, group=None, dst=0, out=None):
     """Forms this rank's block of output rows with compute(a, b, out) (pixel
     rows [a, b) into the float64 tensor out [b - a, nu, 2], on the CUDA
     device for an NCCL group, in host memory for gloo) and gathers the
-    blocks on rank `dst`, which returns the whole image complex128 [nv, nu];
-    the other ranks return None."""
+    blocks on rank `dst`, which returns the whole image complex128 [nv, nu]
+    (in `out` when given, see assemble); the other ranks return None."""
     import torch
     import torch.distributed as dist
     world = dist.get_world_size(group)
@@ -122,7 +130,7 @@ def distributed_backprojection(compute, nu, nv, group=None, dst=0):
     dist.gather(send, gather_list=gather, dst=dst, group=group)
     if rank != dst:
         return None
-    return assemble(gather, nu, nv)
+    return assemble(gather, nu, nv, out)
 
 
 def oracle_compute(backprojection, phs, k_r, taylor_s_l, n_fft, delta_r, u, v, pos, r, **kw):

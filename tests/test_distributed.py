@@ -86,9 +86,16 @@ def _fake_worker(rank, world, port, nu, nv):
         img = distributed_backprojection(compute, nu, nv)
         y0, y1 = output_row_blocks(nv, world)[rank]
         assert calls == ([pixel_rows(nv, y0, y1)] if y1 > y0 else [])
+        want = (nv - 1 - np.arange(nv))[:, None] + 1j * np.arange(nu)[None, :]
         if rank == 0:
-            want = (nv - 1 - np.arange(nv))[:, None] + 1j * np.arange(nu)[None, :]
             assert np.array_equal(img, want)
+        else:
+            assert img is None
+        # again into a caller's buffer on the destination rank, in place
+        out = np.full((nv, nu), np.nan, np.complex128) if rank == 0 else None
+        img = distributed_backprojection(compute, nu, nv, out=out)
+        if rank == 0:
+            assert img is out and np.array_equal(out, want)
         else:
             assert img is None
     finally:
